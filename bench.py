@@ -1,0 +1,335 @@
+"""Benchmark of the render hot path on B200.
+
+Workload (one "step" = one frame): the closed room with the displaced
+81,920-triangle icosphere, 1024 x 1024, 64 spp, depth 10, NEE on, Russian
+roulette from bounce 3, FP32 -- rendered by the persistent megakernel through
+the C ABI. The metric is rays per second with the reference's counting
+convention (one per path segment, one per shadow ray tested).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--mode mega|wave]
+
+With N > 1 (torchrun, one process per GPU) every rank renders its own copy of
+the frame: the path does not shard across GPUs in this workload, so the runs
+are replicas (weak scaling) and value is the sum of all ranks' rays over the
+slowest rank's time. --impl reference times the reference's own CPU renderer
+(oracle/_ref, built from the reference's sources; the C restatement if it is
+absent) on this host's cores on bounded row samples of the same frame.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WIDTH, HEIGHT, SPP, DEPTH, SEED = 1024, 1024, 64, 10, 1
+METRIC = "Mrays/s vs CPU ref"
+WORKLOAD = "room + displaced icosphere (81,920 tris), 1024x1024, 64 spp, depth 10, NEE, RR from bounce 3"
+# Algorithmic bytes per traversal step, fixed by the reference's data sizes:
+# bvh::node 128 B, an order[] entry 4 B, the 36 B a triangle test reads
+# (p0, e1, e2), 16 B per sphere (center, radius), 52 B per instance entered.
+BYTES = np.array([128, 4, 36, 16, 52], np.float64)
+PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
+PROFILE = os.path.join(ROOT, "profiles", "megakernel_room_mesh.json")
+
+
+def peaks():
+    try:
+        with open(PEAKS) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons while the timed region runs."""
+
+    FIELDS = ["clocks.sm", "clocks.max.sm", "power.draw", "clocks_event_reasons.hw_slowdown",
+              "clocks_event_reasons.hw_thermal_slowdown", "clocks_event_reasons.sw_thermal_slowdown",
+              "clocks_event_reasons.sw_power_cap"]
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), "--query-gpu=" + ",".join(self.FIELDS),
+                 "--format=csv,noheader,nounits", "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL,
+                text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) != len(self.FIELDS):
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx.append(float(parts[1]))
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[3:]):
+                if v.lower() in ("active", "1"):
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def bytes_per_ray(desc, cam):
+    """Algorithmic bytes per counted ray from the CPU oracle's traversal
+    counters on a bounded sample of the frame (8 rows at full spp)."""
+    from oracle.oracle import Oracle
+    o = Oracle(desc)
+    rows = [int(HEIGHT * (k + 0.5) / 8) for k in range(8)]
+    totals = np.zeros(5, np.float64)
+    rays = 0
+    for j in rows:
+        _, _, r, c = o.render(cam, WIDTH, HEIGHT, SPP, DEPTH, seed=SEED, rng_mode=0, row0=j, rows=1, counts=True)
+        totals += c
+        rays += r
+    return float((totals * BYTES).sum() / rays), {"rays": int(rays), "rows": rows,
+                                                  "counts": [int(x) for x in totals]}
+
+
+def cpu_reference_rate(desc, cam, seconds: float, threads: int):
+    """The reference renderer (oracle/_ref) on this host's cores, rendering
+    rows of the same frame; returns (Mrays/s, sample description, kind, threads)."""
+    from oracle.oracle import Oracle, Reference, ref_available
+    if ref_available():
+        r, kind = Reference(desc), "reference"
+        run = lambda j0, n: r.render(cam, WIDTH, HEIGHT, SPP, DEPTH, seed=SEED, row0=j0, rows=n, threads=threads)[2]
+    else:
+        o, kind, threads = Oracle(desc), "port", 1
+        run = lambda j0, n: o.render(cam, WIDTH, HEIGHT, SPP, DEPTH, seed=SEED, rng_mode=2, row0=j0, rows=n)[2]
+    t0 = time.perf_counter()
+    rays = run(HEIGHT // 2, max(1, threads // 4))
+    dt = time.perf_counter() - t0
+    rows = int(max(threads, min(HEIGHT, (max(1, threads // 4)) * seconds / max(dt, 1e-3))))
+    j0 = max(0, HEIGHT // 2 - rows // 2)
+    t0 = time.perf_counter()
+    rays = run(j0, rows)
+    dt = time.perf_counter() - t0
+    return rays / dt / 1e6, f"rows {j0}..{j0 + rows - 1} of the 1024x1024 frame at 64 spp ({rays} rays, {dt:.1f} s)", kind, threads
+
+
+def run_reference_arm(args, rank, world):
+    if rank != 0:
+        return 0
+    import photon_tracer_b200 as pt
+    from photon_tracer_b200 import abi
+    from oracle.oracle import Oracle, Reference, ref_available
+    g = pt.Generated(abi.PT_GEN_ROOM_MESH, seed=SEED)
+    threads = os.cpu_count() or 1
+    if ref_available():
+        r, kind = Reference(g.desc), "reference"
+        run = lambda j0, n: r.render(g.camera, WIDTH, HEIGHT, SPP, DEPTH, seed=SEED, row0=j0, rows=n, threads=threads)[2]
+    else:
+        o, kind, threads = Oracle(g.desc), "port", 1
+        run = lambda j0, n: o.render(g.camera, WIDTH, HEIGHT, SPP, DEPTH, seed=SEED, rng_mode=2, row0=j0, rows=n)[2]
+    # size a step to about 4 s of CPU work
+    t0 = time.perf_counter()
+    run(HEIGHT // 2, threads)
+    dt = time.perf_counter() - t0
+    rows = int(max(threads, min(HEIGHT, threads * 4.0 / max(dt, 1e-3))))
+    steps = []
+    for k in range(args.warmup + args.steps):
+        j0 = (k * 131) % max(1, HEIGHT - rows)
+        t0 = time.perf_counter()
+        rays = run(j0, rows)
+        dt = time.perf_counter() - t0
+        if k >= args.warmup:
+            steps.append((rays, dt))
+    rays = sum(s[0] for s in steps)
+    secs = sum(s[1] for s in steps)
+    value = rays / secs / 1e6
+    sample = f"{rows} rows of the 1024x1024 frame at 64 spp per step"
+    line = {"impl": "reference", "metric": METRIC, "value": round(value, 3), "unit": "Mrays/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(secs / len(steps) * 1e3, 3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "scene": "room_mesh", "width": WIDTH, "height": HEIGHT, "spp": SPP,
+                       "depth": DEPTH, "seed": SEED, "rows_per_step": rows},
+            "cpu_baseline": {"value": round(value, 3), "unit": "Mrays/s", "cores": threads, "kind": kind,
+                             "sample": sample},
+            "e2e": {"value": round(value, 3), "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--mode", default="mega", choices=["mega", "wave"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        return run_reference_arm(args, rank, world)
+
+    import torch
+    import torch.distributed as dist
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    import photon_tracer_b200 as pt
+    from photon_tracer_b200 import abi
+
+    g = pt.Generated(abi.PT_GEN_ROOM_MESH, seed=SEED)
+    scene = pt.Scene(g)
+    mode = abi.PT_MODE_MEGAKERNEL if args.mode == "mega" else abi.PT_MODE_WAVEFRONT
+    st = pt.Scene.settings(WIDTH, HEIGHT, SPP, DEPTH, SEED, 0, mode, abi.PT_RNG_SAMPLE)
+    stream = torch.cuda.Stream()
+    out = torch.empty((HEIGHT, WIDTH, 3), dtype=torch.float32, device="cuda")
+    rays_dev = torch.zeros(1, dtype=torch.int64, device="cuda")
+    flush = torch.empty(64 << 20, dtype=torch.float32, device="cuda")  # 256 MB > 126 MB L2
+
+    def step():
+        scene.render_device(g.camera, st, out.data_ptr(), 0, rays_dev.data_ptr(), stream.cuda_stream)
+
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            flush.zero_()
+            step()
+        stream.synchronize()
+        scene.sync(stream.cuda_stream)
+        rays_dev.zero_()
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+        ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+        with ClockSampler(local) as clocks:
+            t_wall = time.perf_counter()
+            for k in range(args.steps):
+                flush.zero_()  # L2 flushed between timed iterations (outside the events)
+                starts[k].record(stream)
+                step()
+                ends[k].record(stream)
+            stream.synchronize()
+            t_wall = time.perf_counter() - t_wall
+        torch.cuda.synchronize()
+        scene.sync(stream.cuda_stream)
+    if world > 1:
+        dist.barrier()
+    times = [s.elapsed_time(e) for s, e in zip(starts, ends)]
+    ms_total = float(sum(times))
+    rays_total = int(rays_dev.item())
+    if world > 1:
+        t = torch.tensor([ms_total], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        r = torch.tensor([rays_total], dtype=torch.int64, device="cuda")
+        dist.all_reduce(r, op=dist.ReduceOp.SUM)
+        ms_total, rays_all = float(t.item()), int(r.item())
+    else:
+        rays_all = rays_total
+    value = rays_all / (ms_total / 1e3) / 1e6
+    rays_per_launch = rays_total / args.steps
+    ms_per_launch = ms_total / args.steps
+
+    # End to end through the public host-buffer call: camera and settings in,
+    # the frame (and ray count) back to host memory, every step.
+    e2e_ms = []
+    img = None
+    for k in range(max(2, min(args.steps, 5))):
+        t0 = time.perf_counter()
+        img, _, rays_e2e = scene.render(g.camera, WIDTH, HEIGHT, SPP, DEPTH, seed=SEED, mode=mode)
+        e2e_ms.append((time.perf_counter() - t0) * 1e3)
+    e2e_value = rays_e2e / (statistics.mean(e2e_ms) / 1e3) / 1e6 * world
+
+    line = None
+    if rank == 0:
+        peak, peak_kind = peaks()
+        bpr, bpr_info = bytes_per_ray(g.desc, g.camera)
+        achieved = bpr * rays_per_launch / (ms_per_launch / 1e3) / 1e9
+        traffic = None
+        if os.path.exists(PROFILE):
+            try:
+                with open(PROFILE) as f:
+                    prof = json.load(f)
+                traffic = prof.get("dram_bytes_per_full_launch")
+            except Exception:
+                traffic = None
+        cpu = None
+        if world == 1 and not args.no_cpu_baseline:
+            rate, sample, kind, threads = cpu_reference_rate(g.desc, g.camera, 10.0, os.cpu_count() or 1)
+            cpu = {"value": round(rate, 3), "unit": "Mrays/s", "cores": threads, "kind": kind, "sample": sample}
+        line = {
+            "metric": METRIC, "value": round(value, 2), "unit": "Mrays/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(ms_per_launch, 3), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "scene": "room_mesh", "triangles": int(g.desc.n_triangles),
+                       "width": WIDTH, "height": HEIGHT, "spp": SPP, "depth": DEPTH, "seed": SEED,
+                       "mode": "megakernel" if mode == abi.PT_MODE_MEGAKERNEL else "wavefront",
+                       "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                       "l2": "flushed between steps (256 MB write, outside the timed events)",
+                       "rays_per_step": int(rays_per_launch), "samples_per_s": round(
+                           WIDTH * HEIGHT * SPP * world / (ms_total / 1e3 / args.steps), 1)},
+            "e2e": {"value": round(e2e_value, 2), "unit": "Mrays/s",
+                    "h2d_bytes_per_step": C.sizeof(abi.pt_camera) + C.sizeof(abi.pt_settings),
+                    "d2h_bytes_per_step": int(img.nbytes) + 8, "api": "pt_render (host buffers)",
+                    "ms_per_step": round(statistics.mean(e2e_ms), 3)},
+            "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                         "frac": round(achieved / peak, 4), "traffic": traffic, "peak_kind": peak_kind,
+                         "bytes_per_ray": round(bpr, 2), "kernel": "megakernel",
+                         "note": "algorithmic bytes = 128*nodes + 4*order + 36*tris + 16*spheres + 52*instances "
+                                 "per ray, counted by the CPU oracle's traversal on 8 rows of the frame; the "
+                                 "scene (~7 MB) is L2-resident, so frac is against HBM but served from L2"},
+            "cpu_baseline": cpu,
+            "gpu_launches": args.steps,
+            "clocks": clocks.summary(),
+            "wall_s_timed_region": round(t_wall, 3),
+        }
+        print(json.dumps(line), flush=True)
+    scene.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,338 @@
+// ref_harness.cpp -- TEST INFRASTRUCTURE, not part of the product.
+//
+// Drives the reference implementation itself: compiled by oracle/build_ref.py
+// against photon_tracer's own headers where they lie (include/*.hpp of the
+// reference checkout), with the reference's Makefile flags (-O3 -std=c++17,
+// no -march) plus -ffp-contract=off, into oracle/_ref/libptref.so. Used by the
+// tests to pin the CPU restatement (pt_oracle.c) and the library's BVH
+// builder, and by bench.py as the reference CPU baseline.
+//
+// Only public members of the reference are used. Where the reference keeps a
+// value private (geometry::hit's choice of primitive, the camera's aspect),
+// the harness re-composes it from public pieces and cross-checks the result
+// against the reference's own call.
+#include <atomic>
+#include <cstring>
+#include <thread>
+#include <vector>
+
+#include "renderer.hpp"
+#include "../include/photon_cuda.h"
+
+namespace {
+
+struct ref_scene {
+    geometry world;
+    std::vector<const material*> mats;
+};
+
+std::shared_ptr<material> material_from(const pt_material& m) {
+    const color albedo(m.albedo[0], m.albedo[1], m.albedo[2]);
+    switch (m.type) {
+        case PT_MAT_LAMBERTIAN: return std::make_shared<lambertian>(albedo);
+        case PT_MAT_METAL: return std::make_shared<metal>(albedo, m.fuzz);
+        case PT_MAT_DIELECTRIC: return std::make_shared<dielectric>(m.ior);
+        default: return std::make_shared<diffuse_light>(color(m.emission[0], m.emission[1], m.emission[2]));
+    }
+}
+
+point3 P(const float* p) { return point3(p[0], p[1], p[2]); }
+
+triangle make_tri(const pt_triangle& t, const material* m) {
+    // The reference's smooth constructor from the corners as given.
+    return triangle(P(t.p0), P(t.p1), P(t.p2), P(t.n0), P(t.n1), P(t.n2), m);
+}
+
+// The camera with its four fields set (the reference's constructor fixes the
+// aspect at 16:9). camera is a standard-layout class of four vec3 in the
+// order origin, lower_left_corner, horizontal, vertical; the accessors check
+// the copy landed where they read.
+camera camera_from(const pt_camera* c) {
+    static_assert(sizeof(camera) == 12 * sizeof(float), "camera layout");
+    camera cam;
+    float f[12];
+    std::memcpy(f, c->origin, 12);
+    std::memcpy(f + 3, c->lower_left, 12);
+    std::memcpy(f + 6, c->horizontal, 12);
+    std::memcpy(f + 9, c->vertical, 12);
+    std::memcpy(static_cast<void*>(&cam), f, sizeof(f));
+    return cam;
+}
+
+}  // namespace
+
+extern "C" {
+
+// Builds the reference geometry for desc (trees built by geometry::build).
+void* ref_scene_create(const pt_scene_desc* d) {
+    auto* s = new ref_scene();
+    geometry& w = s->world;
+    for (uint32_t i = 0; i < d->n_materials; ++i) s->mats.push_back(w.own(material_from(d->materials[i])));
+    for (uint32_t i = 0; i < d->n_spheres; ++i) {
+        const pt_sphere& sp = d->spheres[i];
+        w.spheres.emplace_back(P(sp.center), sp.radius, s->mats[sp.material]);
+    }
+    for (uint32_t i = 0; i < d->n_large_spheres; ++i) {
+        const pt_sphere& sp = d->large_spheres[i];
+        w.large_spheres.emplace_back(P(sp.center), sp.radius, s->mats[sp.material]);
+    }
+    for (uint32_t i = 0; i < d->n_triangles; ++i)
+        w.triangles.push_back(make_tri(d->triangles[i], s->mats[d->triangles[i].material]));
+    for (uint32_t m = 0; m < d->n_meshes; ++m) {
+        std::vector<triangle> tris;
+        for (uint32_t i = 0; i < d->meshes[m].n_triangles; ++i)
+            tris.push_back(make_tri(d->meshes[m].triangles[i], s->mats[d->meshes[m].triangles[i].material]));
+        w.add_mesh(std::move(tris));
+    }
+    for (uint32_t k = 0; k < d->n_instances; ++k) {
+        const pt_instance& in = d->instances[k];
+        affine x;
+        for (int r = 0; r < 3; ++r) {
+            for (int c = 0; c < 3; ++c) x.m[r][c] = in.to_world.m[r][c];
+            x.t.e[r] = in.to_world.t[r];
+        }
+        w.add_instance(in.mesh, x, in.material == PT_NO_MATERIAL ? nullptr : s->mats[in.material]);
+    }
+    w.sky = d->sky != 0;
+    w.sample_lights = d->sample_lights != 0;
+    w.build(d->use_bvh != 0);
+    return s;
+}
+
+void ref_scene_destroy(void* h) { delete static_cast<ref_scene*>(h); }
+
+// Copies the fields the reference's constructors computed, for comparison
+// with the description (e1, e2, face normal per triangle; to_object per instance).
+void ref_triangle_fields(void* h, int mesh, uint32_t i, float out[12]) {
+    const geometry& w = static_cast<ref_scene*>(h)->world;
+    const triangle& t = mesh < 0 ? w.triangles[i] : w.meshes[mesh].triangles[i];
+    const vec3 v[4] = {t.p0, t.e1, t.e2, t.face_normal};
+    for (int k = 0; k < 4; ++k)
+        for (int a = 0; a < 3; ++a) out[3 * k + a] = v[k].e[a];
+}
+
+void ref_instance_to_object(void* h, uint32_t k, float out[12]) {
+    const geometry& w = static_cast<ref_scene*>(h)->world;
+    const affine& x = w.instances[k].to_object;
+    for (int r = 0; r < 3; ++r) {
+        for (int c = 0; c < 3; ++c) out[3 * r + c] = x.m[r][c];
+        out[9 + r] = x.t.e[r];
+    }
+}
+
+// A tree the reference built: which 0 = flat, 1 = instances, 2 = mesh `mesh`.
+// Returns the node count; copies when the buffers are large enough.
+uint32_t ref_tree(void* h, int which, int mesh, pt_bvh_node* nodes, uint32_t cap_nodes, uint32_t* order,
+                  uint32_t cap_order, uint32_t* n_order) {
+    const geometry& w = static_cast<ref_scene*>(h)->world;
+    const bvh& t = which == 0 ? w.flat_tree() : which == 1 ? w.instances_tree() : w.meshes[mesh].tree;
+    static_assert(sizeof(bvh::node) == sizeof(pt_bvh_node), "node layout");
+    if (nodes && cap_nodes >= t.nodes.size()) std::memcpy(nodes, t.nodes.data(), t.nodes.size() * sizeof(pt_bvh_node));
+    if (order && cap_order >= t.order.size()) std::memcpy(order, t.order.data(), t.order.size() * sizeof(uint32_t));
+    *n_order = uint32_t(t.order.size());
+    return uint32_t(t.nodes.size());
+}
+
+// geometry::hit's choice of primitive, re-composed from the public trees with
+// the lambdas of geometry.hpp:117-139 and hit_instance :212-229, and checked
+// against geometry::hit itself: *mismatch counts rays where rec.t or rec.p differ.
+void ref_trace_closest(void* h, const float* rays, size_t n, float t_min, float t_max_in, pt_hit* out,
+                       uint64_t* mismatch) {
+    const geometry& w = static_cast<ref_scene*>(h)->world;
+    uint64_t bad = 0;
+    for (size_t q = 0; q < n; ++q) {
+        const float* rr = rays + 6 * q;
+        const ray r(point3(rr[0], rr[1], rr[2]), vec3(rr[3], rr[4], rr[5]));
+        real t_max = t_max_in;
+        uint32_t kind = PT_HIT_NONE, index = 0, sub = 0;
+        real u = 0, v = 0;
+        for (uint32_t i = 0; i < w.large_spheres.size(); ++i)
+            if (w.large_spheres[i].intersect<double>(r, t_min, t_max)) { kind = PT_HIT_LARGE; index = i; }
+        const uint32_t ns = uint32_t(w.spheres.size());
+        auto test = [&](uint32_t p, real& t_far) {
+            if (p < ns) {
+                if (w.spheres[p].intersect(r, t_min, t_far)) { kind = PT_HIT_SPHERE; index = p; }
+            } else if (w.triangles[p - ns].intersect(r, t_min, t_far, u, v)) {
+                kind = PT_HIT_TRIANGLE; index = p - ns;
+            }
+        };
+        auto test_instance = [&](uint32_t k, real& t_far) {
+            const geometry::instance& in = w.instances[k];
+            const geometry::mesh& m = w.meshes[in.mesh];
+            const ray local(in.to_object.point(r.origin()), in.to_object.vector(r.direction()));
+            bool found = false;
+            real ht = t_far, hu = 0, hv = 0;
+            uint32_t tri = 0;
+            m.tree.traverse(local, t_min, ht, [&](uint32_t ti, real& t_mesh) {
+                if (m.triangles[ti].intersect(local, t_min, t_mesh, hu, hv)) { found = true; tri = ti; }
+            });
+            if (found) { kind = PT_HIT_INSTANCE; index = k; t_far = ht; u = hu; v = hv; sub = tri; }
+        };
+        if (w.uses_bvh()) {
+            w.flat_tree().traverse(r, t_min, t_max, test);
+            if (!w.instances.empty()) w.instances_tree().traverse(r, t_min, t_max, test_instance);
+        } else {
+            const uint32_t np = ns + uint32_t(w.triangles.size());
+            for (uint32_t p = 0; p < np; ++p) test(p, t_max);
+            for (uint32_t k = 0; k < w.instances.size(); ++k) test_instance(k, t_max);
+        }
+        hit_record rec;
+        const bool got = w.hit(r, t_min, t_max_in, rec);
+        if (got != (kind != PT_HIT_NONE)) ++bad;
+        else if (got) {
+            const point3 p = r.at(t_max);
+            if (rec.t != t_max || rec.p.e[0] != p.e[0] || rec.p.e[1] != p.e[1] || rec.p.e[2] != p.e[2]) ++bad;
+        }
+        out[q].kind = kind;
+        out[q].index = kind == PT_HIT_NONE ? 0 : index;
+        out[q].sub = sub;
+        out[q].t = t_max;
+        out[q].u = u;
+        out[q].v = v;
+    }
+    *mismatch = bad;
+}
+
+void ref_trace_any(void* h, const float* rays, size_t n, float t_min, float t_max, uint8_t* out) {
+    const geometry& w = static_cast<ref_scene*>(h)->world;
+    for (size_t q = 0; q < n; ++q) {
+        const float* rr = rays + 6 * q;
+        out[q] = w.occluded(ray(point3(rr[0], rr[1], rr[2]), vec3(rr[3], rr[4], rr[5])), t_min, t_max) ? 1 : 0;
+    }
+}
+
+// render_row_linear over scanlines [row0, row0 + rows) on `threads` threads
+// taking rows from an atomic counter (src/main.cpp:137-158), written in
+// pt_render's layout (top row first; aux 7 floats or NULL). Returns the ray
+// count (include/renderer.hpp:19, summed as main.cpp:157 does).
+uint64_t ref_render(void* h, const pt_camera* c, int W, int H, int spp, int depth, uint64_t seed, int first_sample,
+                    int row0, int rows, float* out, float* aux, int threads) {
+    const geometry& w = static_cast<ref_scene*>(h)->world;
+    const camera cam = camera_from(c);
+    std::atomic<int> next{row0};
+    std::atomic<long long> total{0};
+    auto worker = [&]() {
+        rays_traced = 0;
+        for (int j = next.fetch_add(1); j < row0 + rows; j = next.fetch_add(1)) {
+            const size_t row = size_t(H - 1 - j) * W;
+            render_row_linear(w, cam, j, W, H, spp, depth, out + 3 * row, seed, first_sample,
+                              aux ? aux + aux_floats * row : nullptr);
+        }
+        total += rays_traced;
+    };
+    if (threads <= 1) {
+        worker();
+    } else {
+        std::vector<std::thread> pool;
+        for (int t = 0; t < threads; ++t) pool.emplace_back(worker);
+        for (auto& t : pool) t.join();
+    }
+    return uint64_t(total.load());
+}
+
+// render_row_impl's loop (include/renderer.hpp:370-396) with the reference's
+// own seed_row stream, capturing thread_rng's state before each ray_color:
+// states gets 4 words per (pixel, sample), pixels row by row from j = row0,
+// as PT_RNG_SNAPSHOT reads them. Writes the image like ref_render.
+uint64_t ref_render_snapshot(void* h, const pt_camera* c, int W, int H, int spp, int depth, uint64_t seed,
+                             int first_sample, int row0, int rows, float* out, float* aux, uint64_t* states) {
+    const geometry& w = static_cast<ref_scene*>(h)->world;
+    const camera cam = camera_from(c);
+    rays_traced = 0;
+    for (int j = row0; j < row0 + rows; ++j) {
+        seed_row(seed, j, first_sample);
+        const real scale = real(1) / spp;
+        for (int i = 0; i < W; ++i) {
+            color pc(0, 0, 0), albedo(0, 0, 0);
+            vec3 normal(0, 0, 0);
+            real lum2 = 0;
+            for (int s = 0; s < spp; ++s) {
+                begin_sample(seed, i, j, static_cast<uint32_t>(first_sample + s));
+                real du, dv;
+                sample_2d(0, du, dv);
+                const ray r = cam.get_ray((i + du) / (W - 1), (j + dv) / (H - 1));
+                std::memcpy(states + 4 * ((size_t(j - row0) * W + i) * spp + s), thread_rng.s, 32);
+                first_hit first;
+                const color col = ray_color<true>(r, w, depth, &first);
+                pc = pc + col;
+                albedo = albedo + first.albedo;
+                normal = normal + first.normal;
+                lum2 += luminance(col) * luminance(col);
+            }
+            const size_t px = size_t(H - 1 - j) * W + i;
+            for (int k = 0; k < 3; ++k) out[3 * px + k] = static_cast<float>(pc.e[k] * scale);
+            if (aux) {
+                for (int k = 0; k < 3; ++k) {
+                    aux[7 * px + k] = static_cast<float>(albedo.e[k] * scale);
+                    aux[7 * px + 3 + k] = static_cast<float>(normal.e[k] * scale);
+                }
+                aux[7 * px + 6] = static_cast<float>(lum2 * scale);
+            }
+        }
+    }
+    return uint64_t(rays_traced);
+}
+
+// The reference's denoiser (include/denoise.hpp:55-139).
+void ref_denoise(int w, int h, const float* color, const float* albedo, const float* normal, const float* variance,
+                 float* out, int threads) {
+    denoise({w, h, color, albedo, normal, variance}, out, threads);
+}
+
+// The reference's sampler, for known-answer checks: (a, b) of pair_offset
+// at the given bounce (-1: before any set_bounce) for sample index of pixel (i, j).
+void ref_sample_2d(uint64_t seed, int i, int j, uint32_t index, int bounce, int pair_offset, float out[2]) {
+    begin_sample(seed, i, j, index);
+    if (bounce >= 0) set_bounce(bounce);
+    thread_rng.seed(1);
+    real a, b;
+    sample_2d(pair_offset, a, b);
+    out[0] = a;
+    out[1] = b;
+}
+
+// The camera the reference builds (16:9) for a lookfrom/lookat/vfov.
+void ref_camera(const float from[3], const float at[3], double vfov, pt_camera* out) {
+    const camera c(point3(from[0], from[1], from[2]), point3(at[0], at[1], at[2]), vfov);
+    for (int a = 0; a < 3; ++a) {
+        out->origin[a] = c.position().e[a];
+        out->lower_left[a] = c.corner().e[a];
+        out->horizontal[a] = c.across().e[a];
+        out->vertical[a] = c.up().e[a];
+    }
+}
+
+// Checks make_camera's layout assumption: the accessors of the copied camera.
+int ref_camera_roundtrip(const pt_camera* c) {
+    const camera cam = camera_from(c);
+    for (int a = 0; a < 3; ++a)
+        if (cam.position().e[a] != c->origin[a] || cam.corner().e[a] != c->lower_left[a] ||
+            cam.across().e[a] != c->horizontal[a] || cam.up().e[a] != c->vertical[a])
+            return 0;
+    return 1;
+}
+
+// The reference's own scenes, for comparing with the library's generators:
+// fills counts {spheres, large, triangles, materials} and copies spheres
+// (center, radius) and triangles (p0, e1, e2) when buffers are given.
+void ref_builtin_scene(int id, uint32_t counts[4], float* spheres, float* tris) {
+    const geometry w = build_world(static_cast<scene_id>(id), true);
+    counts[0] = uint32_t(w.spheres.size());
+    counts[1] = uint32_t(w.large_spheres.size());
+    counts[2] = uint32_t(w.triangles.size());
+    counts[3] = 0;
+    if (spheres)
+        for (size_t i = 0; i < w.spheres.size(); ++i) {
+            for (int a = 0; a < 3; ++a) spheres[4 * i + a] = w.spheres[i].center.e[a];
+            spheres[4 * i + 3] = w.spheres[i].radius;
+        }
+    if (tris)
+        for (size_t i = 0; i < w.triangles.size(); ++i)
+            for (int a = 0; a < 3; ++a) {
+                tris[9 * i + a] = w.triangles[i].p0.e[a];
+                tris[9 * i + 3 + a] = w.triangles[i].e1.e[a];
+                tris[9 * i + 6 + a] = w.triangles[i].e2.e[a];
+            }
+}
+
+}  // extern "C"

@@ -1,0 +1,46 @@
+// Launch interface between the host glue (api.cpp) and the kernels (*.cu).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "pt_layout.h"
+
+struct PtCamDev {
+    float origin[3], llc[3], horizontal[3], vertical[3];
+};
+
+// One render launch: scanlines [row0, row0 + rows) of a width x height image.
+// Scanline j lands in output row (flip ? height - 1 - j : j - row0).
+struct PtRenderParams {
+    PtCamDev cam;
+    int width, height, spp, depth;
+    uint64_t seed;
+    int first_sample;
+    int rng_mode;               // PT_RNG_*
+    const uint64_t* states;     // PT_RNG_SNAPSHOT: per (pixel, sample) xoshiro state
+    int row0, rows, flip;
+    float* out;                 // 3 floats per pixel
+    float* aux;                 // 7 floats per pixel or null
+    unsigned long long* rays;   // one counter the launch adds its rays to (may be null)
+    unsigned int* work;         // one zeroed work counter (megakernel)
+};
+
+// Sizing of persistent launches.
+struct PtLaunchShape {
+    int blocks, threads;
+};
+
+// Megakernel: persistent warps take pixels from a global counter; each lane
+// renders its pixel's samples one path after another.
+cudaError_t pt_launch_megakernel(const PtSceneDev& scene, const PtRenderParams& p, const PtLaunchShape& shape,
+                                 cudaStream_t stream);
+int pt_megakernel_blocks_per_sm(int threads, bool aux, bool snapshot);
+
+// Ray queries: closest hit (pt_hit records), any hit (bytes), and traversal
+// work counters (5 x u64, added to).
+cudaError_t pt_launch_trace_closest(const PtSceneDev& scene, const float* rays, size_t n, float tmin, float tmax,
+                                    void* hits, cudaStream_t stream);
+cudaError_t pt_launch_trace_any(const PtSceneDev& scene, const float* rays, size_t n, float tmin, float tmax,
+                                uint8_t* occluded, cudaStream_t stream);
+cudaError_t pt_launch_trace_count(const PtSceneDev& scene, const float* rays, size_t n, float tmin, float tmax,
+                                  unsigned long long* counts, cudaStream_t stream);

@@ -1,0 +1,199 @@
+// Persistent-thread megakernel path tracer.
+//
+// The CPU renderer gives each thread a whole scanline, taken from an atomic
+// row counter (src/main.cpp:137-158), and runs samples_per_pixel paths per
+// pixel one after another (include/renderer.hpp:366-409). Here each LANE owns
+// a pixel, runs its samples one path after another (so the per-pixel sums
+// are formed in the same order as the reference's), and advances one bounce
+// per loop trip; when its pixel is finished it takes the next from a global
+// counter, warp-aggregated (one atomicAdd per warp per refill). Pixels are
+// numbered by 8x4 tiles so a warp's first pixels are neighbours and their
+// primary rays coherent. Work per warp is therefore balanced at path
+// granularity and no lane waits for another lane's pixel.
+#include "kernels.h"
+#include "path.cuh"
+
+using namespace ptd;
+
+namespace {
+
+constexpr int kTileW = 8, kTileH = 4;
+
+template <bool AUX, bool SNAP>
+__global__ void __launch_bounds__(128) megakernel(PtSceneDev S, PtRenderParams P, uint32_t tiles_x,
+                                                  uint32_t total_items) {
+    StackEntry stack[PT_STACK_MAX];
+    const int lane = threadIdx.x & 31;
+    const Cam cam = {mk(P.cam.origin[0], P.cam.origin[1], P.cam.origin[2]),
+                     mk(P.cam.llc[0], P.cam.llc[1], P.cam.llc[2]),
+                     mk(P.cam.horizontal[0], P.cam.horizontal[1], P.cam.horizontal[2]),
+                     mk(P.cam.vertical[0], P.cam.vertical[1], P.cam.vertical[2])};
+    const float scale = 1.0f / float(P.spp);
+    const float wm1 = float(P.width - 1), hm1 = float(P.height - 1);
+
+    unsigned long long rays = 0;
+    bool exhausted = false, has_pixel = false, in_path = false;
+    int pi = 0, pj = 0, s = 0;
+    V acc = mk(0, 0, 0), acc_albedo = mk(0, 0, 0), acc_normal = mk(0, 0, 0);
+    float lum2 = 0;
+    Path path;
+    First first = {mk(0, 0, 0), mk(0, 0, 0)};
+    Sampler smp;
+    Rng rng;
+    bool overflow = false;
+
+    while (true) {
+        // Refill lanes without a pixel.
+        const bool need = !has_pixel && !exhausted;
+        const unsigned want = __ballot_sync(0xffffffffu, need);
+        if (want) {
+            const int leader = __ffs(want) - 1;
+            uint32_t base = 0;
+            if (lane == leader) base = atomicAdd(P.work, uint32_t(__popc(want)));
+            base = __shfl_sync(0xffffffffu, base, leader);
+            if (need) {
+                const uint32_t item = base + __popc(want & ((1u << lane) - 1u));
+                if (item >= total_items) {
+                    exhausted = true;
+                } else {
+                    const uint32_t tile = item >> 5, l = item & 31u;
+                    pi = int((tile % tiles_x) * kTileW + (l & 7u));
+                    pj = P.row0 + int((tile / tiles_x) * kTileH + (l >> 3));
+                    if (pi < P.width && pj < P.row0 + P.rows) {
+                        has_pixel = true;
+                        s = 0;
+                        in_path = false;
+                        acc = acc_albedo = acc_normal = mk(0, 0, 0);
+                        lum2 = 0;
+                    }
+                }
+            }
+        }
+        if (__all_sync(0xffffffffu, exhausted)) break;
+        if (!has_pixel) continue;
+
+        if (!in_path) {
+            if (P.depth <= 0 || P.spp <= 0) {
+                s = P.spp;  // nothing to trace: every sample is black
+            } else {
+                // render_row_impl's sample loop body (:379-385)
+                const uint32_t idx = uint32_t(P.first_sample + s);
+                smp.begin(P.seed, pi, pj, idx);
+                float du, dv;
+                smp.sample_2d(0, rng, du, dv);
+                const float u = (float(pi) + du) / wm1;
+                const float v = (float(pj) + dv) / hm1;
+                path.o = cam.origin;
+                path.d = cam.llc + cam.horizontal * u + cam.vertical * v - cam.origin;
+                path.tp = mk(1, 1, 1);
+                path.rad = mk(0, 0, 0);
+                path.bounce = 0;
+                path.sampled = false;
+                first = {mk(0, 0, 0), mk(0, 0, 0)};
+                if (SNAP) {
+                    const uint64_t* st = P.states + 4 * ((size_t(pj) * P.width + pi) * P.spp + s);
+                    rng.s0 = st[0];
+                    rng.s1 = st[1];
+                    rng.s2 = st[2];
+                    rng.s3 = st[3];
+                } else {
+                    rng.seed(sample_stream_seed(P.seed, pi, pj, idx));
+                }
+                in_path = true;
+            }
+        }
+
+        if (in_path) {
+            // One iteration of ray_color's bounce loop.
+            ++rays;
+            smp.set_bounce(path.bounce);
+            float t = 1000.0f;
+            Hit h;
+            Counts cnt;
+            Rec rec;
+            bool ok = closest<false>(S, path.o, path.d, 0.001f, t, h, stack, cnt);
+            if (!ok) {
+                overflow = true;
+                h.kind = PT_HIT_NONE;
+            }
+            const bool hit = h.kind != PT_HIT_NONE;
+            if (hit) fill(S, h, path.o, path.d, t, rec);
+            bool nee;
+            Shadow sh;
+            const int step = shade<AUX>(S, path, hit, rec, P.depth, smp, rng, first, nee, sh, rays);
+            if (nee) {
+                bool ovf = false;
+                if (!occluded<false>(S, sh.o, sh.d, 0.001f, sh.t_max, stack, cnt, &ovf))
+                    path.rad = path.rad + sh.value;
+                overflow |= ovf;
+            }
+            if (step == STEP_DONE) {
+                acc = acc + path.rad;
+                if (AUX) {
+                    acc_albedo = acc_albedo + first.albedo;
+                    acc_normal = acc_normal + first.normal;
+                    const float l = luminance(path.rad);
+                    lum2 += l * l;
+                }
+                in_path = false;
+                ++s;
+            }
+        }
+
+        if (s >= P.spp) {
+            const int row = P.flip ? (P.height - 1 - pj) : (pj - P.row0);
+            const size_t px = size_t(row) * P.width + pi;
+            P.out[3 * px + 0] = acc.x * scale;
+            P.out[3 * px + 1] = acc.y * scale;
+            P.out[3 * px + 2] = acc.z * scale;
+            if (AUX) {
+                float* a = P.aux + 7 * px;
+                a[0] = acc_albedo.x * scale;
+                a[1] = acc_albedo.y * scale;
+                a[2] = acc_albedo.z * scale;
+                a[3] = acc_normal.x * scale;
+                a[4] = acc_normal.y * scale;
+                a[5] = acc_normal.z * scale;
+                a[6] = lum2 * scale;
+            }
+            has_pixel = false;
+        }
+    }
+
+    // Ray count: warp sum, one atomic per warp.
+    unsigned long long total = rays;
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) total += __shfl_down_sync(0xffffffffu, total, off);
+    if (lane == 0 && P.rays) atomicAdd(P.rays, total);
+    if (__any_sync(0xffffffffu, overflow) && lane == 0) atomicOr(S.status, PT_DEV_ERR_STACK);
+}
+
+template <bool AUX, bool SNAP>
+cudaError_t launch(const PtSceneDev& S, const PtRenderParams& p, const PtLaunchShape& shape, cudaStream_t stream) {
+    const uint32_t tiles_x = uint32_t((p.width + kTileW - 1) / kTileW);
+    const uint32_t tiles_y = uint32_t((p.rows + kTileH - 1) / kTileH);
+    const uint32_t total = tiles_x * tiles_y * 32u;
+    megakernel<AUX, SNAP><<<shape.blocks, shape.threads, 0, stream>>>(S, p, tiles_x, total);
+    return cudaGetLastError();
+}
+
+template <bool AUX, bool SNAP>
+int occupancy(int threads) {
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, megakernel<AUX, SNAP>, threads, 0) != cudaSuccess) n = 1;
+    return n > 0 ? n : 1;
+}
+
+}  // namespace
+
+cudaError_t pt_launch_megakernel(const PtSceneDev& S, const PtRenderParams& p, const PtLaunchShape& shape,
+                                 cudaStream_t stream) {
+    const bool aux = p.aux != nullptr, snap = p.rng_mode == 1;
+    if (aux) return snap ? launch<true, true>(S, p, shape, stream) : launch<true, false>(S, p, shape, stream);
+    return snap ? launch<false, true>(S, p, shape, stream) : launch<false, false>(S, p, shape, stream);
+}
+
+int pt_megakernel_blocks_per_sm(int threads, bool aux, bool snapshot) {
+    if (aux) return snapshot ? occupancy<true, true>(threads) : occupancy<true, false>(threads);
+    return snapshot ? occupancy<false, true>(threads) : occupancy<false, false>(threads);
+}

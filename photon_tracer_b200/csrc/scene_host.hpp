@@ -1,0 +1,33 @@
+// The host-side image of the device arena (pt_layout.h), built by build_arena
+// and uploaded as is.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <array>
+#include <vector>
+
+#include "pt_host.hpp"
+#include "pt_layout.h"
+
+namespace pt {
+
+struct HostArena {
+    std::vector<float> nodes;   // 32 floats per node
+    std::vector<float> slots;   // 12 floats per slot
+    std::vector<float> islots;  // 16 floats per instance slot
+    std::vector<float4> large;
+    std::vector<uint32_t> large_mat;
+    std::vector<PtShadeSphere> sph;
+    std::vector<PtShadeTri> tri;
+    std::vector<PtShadeInst> inst;
+    std::vector<PtMaterial> mat;
+    std::vector<PtLight> lights;
+    uint32_t flat_root = PT_NONE, inst_root = PT_NONE;
+    uint32_t n_flat_slots = 0, n_instances = 0, n_spheres = 0;
+    uint32_t stack_entries = 0, max_depth = 0;
+    int sky = 1, sample_lights = 1, use_bvh = 1;
+};
+
+pt_status build_arena(const pt_scene_desc& d, HostArena& A);
+
+}  // namespace pt

@@ -1,0 +1,115 @@
+// Ray-query kernels: closest hit and any hit for caller-supplied rays (one
+// thread per ray), and the same closest-hit traversal instrumented to count
+// the work the algorithmic-bytes roofline is defined on.
+#include "../../include/photon_cuda.h"
+#include "kernels.h"
+#include "tracer.cuh"
+
+using namespace ptd;
+
+namespace {
+
+__device__ __forceinline__ void load_ray(const float* rays, size_t i, V& o, V& d) {
+    const float* r = rays + 6 * i;
+    o = mk(r[0], r[1], r[2]);
+    d = mk(r[3], r[4], r[5]);
+}
+
+__global__ void __launch_bounds__(128) trace_closest_kernel(PtSceneDev S, const float* __restrict__ rays, size_t n,
+                                                             float tmin, float tmax, pt_hit* __restrict__ hits) {
+    StackEntry stack[PT_STACK_MAX];
+    bool overflow = false;
+    for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x) {
+        V o, d;
+        load_ray(rays, i, o, d);
+        float t = tmax;
+        Hit h;
+        Counts cnt;
+        if (!closest<false>(S, o, d, tmin, t, h, stack, cnt)) {
+            overflow = true;
+            h.kind = PT_HIT_NONE;
+        }
+        uint32_t index, sub;
+        resolve(S, h, index, sub);
+        pt_hit out;
+        out.kind = h.kind;
+        out.index = h.kind == PT_HIT_NONE ? 0u : index;
+        out.sub = sub;
+        out.t = t;
+        out.u = h.u;
+        out.v = h.v;
+        hits[i] = out;
+    }
+    if (overflow) atomicOr(S.status, PT_DEV_ERR_STACK);
+}
+
+__global__ void __launch_bounds__(128) trace_any_kernel(PtSceneDev S, const float* __restrict__ rays, size_t n,
+                                                         float tmin, float tmax, uint8_t* __restrict__ occ) {
+    StackEntry stack[PT_STACK_MAX];
+    bool overflow = false;
+    for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x) {
+        V o, d;
+        load_ray(rays, i, o, d);
+        Counts cnt;
+        bool ovf = false;
+        const bool b = occluded<false>(S, o, d, tmin, tmax, stack, cnt, &ovf);
+        overflow |= ovf;
+        occ[i] = b ? 1 : 0;
+    }
+    if (overflow) atomicOr(S.status, PT_DEV_ERR_STACK);
+}
+
+__global__ void __launch_bounds__(128) trace_count_kernel(PtSceneDev S, const float* __restrict__ rays, size_t n,
+                                                           float tmin, float tmax,
+                                                           unsigned long long* __restrict__ counts) {
+    StackEntry stack[PT_STACK_MAX];
+    Counts cnt = {0, 0, 0, 0, 0};
+    bool overflow = false;
+    for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x) {
+        V o, d;
+        load_ray(rays, i, o, d);
+        float t = tmax;
+        Hit h;
+        if (!closest<true>(S, o, d, tmin, t, h, stack, cnt)) overflow = true;
+    }
+    unsigned long long v[5] = {cnt.nodes, cnt.order, cnt.tris, cnt.spheres, cnt.insts};
+#pragma unroll
+    for (int k = 0; k < 5; ++k) {
+        unsigned long long x = v[k];
+        for (int off = 16; off > 0; off >>= 1) x += __shfl_down_sync(0xffffffffu, x, off);
+        if ((threadIdx.x & 31) == 0) atomicAdd(counts + k, x);
+    }
+    if (overflow) atomicOr(S.status, PT_DEV_ERR_STACK);
+}
+
+int grid_for(size_t n, int threads) {
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const size_t want = (n + threads - 1) / threads;
+    const size_t cap = size_t(sms) * 16;
+    return int(want < cap ? (want ? want : 1) : cap);
+}
+
+}  // namespace
+
+cudaError_t pt_launch_trace_closest(const PtSceneDev& S, const float* rays, size_t n, float tmin, float tmax,
+                                    void* hits, cudaStream_t stream) {
+    if (n == 0) return cudaSuccess;
+    trace_closest_kernel<<<grid_for(n, 128), 128, 0, stream>>>(S, rays, n, tmin, tmax, static_cast<pt_hit*>(hits));
+    return cudaGetLastError();
+}
+
+cudaError_t pt_launch_trace_any(const PtSceneDev& S, const float* rays, size_t n, float tmin, float tmax,
+                                uint8_t* occ, cudaStream_t stream) {
+    if (n == 0) return cudaSuccess;
+    trace_any_kernel<<<grid_for(n, 128), 128, 0, stream>>>(S, rays, n, tmin, tmax, occ);
+    return cudaGetLastError();
+}
+
+cudaError_t pt_launch_trace_count(const PtSceneDev& S, const float* rays, size_t n, float tmin, float tmax,
+                                  unsigned long long* counts, cudaStream_t stream) {
+    if (n == 0) return cudaSuccess;
+    trace_count_kernel<<<grid_for(n, 128), 128, 0, stream>>>(S, rays, n, tmin, tmax, counts);
+    return cudaGetLastError();
+}

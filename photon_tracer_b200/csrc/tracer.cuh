@@ -1,0 +1,654 @@
+// Device side of the render hot path: BVH4 traversal, sphere and triangle
+// intersection, hit records, the Sobol/xoshiro sampler and the materials.
+//
+// Every float expression is written in the reference's evaluation order and
+// this file is compiled with -fmad=false -prec-div=true -prec-sqrt=true, so
+// closest hits (primitive, t, u, v) are bit-identical to the reference's
+// geometry::hit on the same rays. The comments cite the reference function
+// each routine restates (photon_tracer, include/...).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/photon_cuda.h"
+#include "pt_layout.h"
+
+namespace ptd {
+
+// ---- float3 helpers in the reference's order (include/vec3.hpp:71-118) --------------
+struct V {
+    float x, y, z;
+};
+__device__ __forceinline__ V mk(float x, float y, float z) { return {x, y, z}; }
+__device__ __forceinline__ V operator+(V a, V b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
+__device__ __forceinline__ V operator-(V a, V b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+__device__ __forceinline__ V operator-(V a) { return {-a.x, -a.y, -a.z}; }
+__device__ __forceinline__ V operator*(V a, V b) { return {a.x * b.x, a.y * b.y, a.z * b.z}; }
+__device__ __forceinline__ V operator*(V a, float t) { return {a.x * t, a.y * t, a.z * t}; }
+__device__ __forceinline__ float dot(V a, V b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__device__ __forceinline__ V cross(V a, V b) {
+    return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+}
+// vec3::normalize divides each component by the length (vec3.hpp:95-98).
+__device__ __forceinline__ V normalize(V a) {
+    const float len = sqrtf(a.x * a.x + a.y * a.y + a.z * a.z);
+    return {a.x / len, a.y / len, a.z / len};
+}
+// vec3::operator/ multiplies by the reciprocal (vec3.hpp:87-89).
+__device__ __forceinline__ V div(V a, float t) { return a * (1.0f / t); }
+__device__ __forceinline__ V xyz(float4 f) { return {f.x, f.y, f.z}; }
+
+// SSE minps / maxps (include/simd4.hpp:15-16): the second operand unless the
+// first compares strictly less / greater, which also decides NaNs.
+__device__ __forceinline__ float sse_min(float a, float b) { return a < b ? a : b; }
+__device__ __forceinline__ float sse_max(float a, float b) { return a > b ? a : b; }
+
+__device__ __forceinline__ uint32_t fbits(float f) { return __float_as_uint(f); }
+
+// ---- hits --------------------------------------------------------------------------------
+struct Hit {
+    uint32_t kind;   // PT_HIT_*
+    uint32_t index;  // slot (flat / mesh) or large sphere number, resolved later
+    uint32_t inst;   // instance number for instance hits
+    float u, v;
+};
+
+// Work counters for the algorithmic-bytes roofline (nodes, leaf entries,
+// triangles, spheres, instances).
+struct Counts {
+    uint32_t nodes, order, tris, spheres, insts;
+};
+
+struct StackEntry {
+    uint32_t first, count;
+    float t;
+    uint32_t pad;
+};
+
+// ---- primitives ------------------------------------------------------------------------
+// sphere::intersect<float> (include/sphere.hpp:25-48).
+__device__ __forceinline__ bool sphere_hit(float4 cr, V o, V d, float t_min, float& t_max) {
+    const float ox = o.x - cr.x, oy = o.y - cr.y, oz = o.z - cr.z;
+    const float a = d.x * d.x + d.y * d.y + d.z * d.z;
+    const float half_b = ox * d.x + oy * d.y + oz * d.z;
+    const float c = ox * ox + oy * oy + oz * oz - cr.w * cr.w;
+    const float disc = half_b * half_b - a * c;
+    if (disc < 0) return false;
+    const float sqrtd = sqrtf(disc);
+    float root = (-half_b - sqrtd) / a;
+    if (root < t_min || root > t_max) {
+        root = (-half_b + sqrtd) / a;
+        if (root < t_min || root > t_max) return false;
+    }
+    t_max = root;
+    return true;
+}
+
+// sphere::intersect<double> (include/sphere.hpp:25-48 with P = double), the
+// test geometry::hit and occluded use for large spheres (include/geometry.hpp:117-118,
+// 157-160). The only double arithmetic in the traversal: it is what makes the
+// t of a ray bouncing off a radius-1000 ground exact.
+__device__ __forceinline__ bool sphere_hit_double(float4 cr, V o, V d, float t_min, float& t_max) {
+    const double ox = double(o.x) - double(cr.x), oy = double(o.y) - double(cr.y), oz = double(o.z) - double(cr.z);
+    const double dx = d.x, dy = d.y, dz = d.z;
+    const double a = dx * dx + dy * dy + dz * dz;
+    const double half_b = ox * dx + oy * dy + oz * dz;
+    const double c = ox * ox + oy * oy + oz * oz - double(cr.w) * double(cr.w);
+    const double disc = half_b * half_b - a * c;
+    if (disc < 0) return false;
+    const double sqrtd = sqrt(disc);
+    double root = (-half_b - sqrtd) / a;
+    if (root < double(t_min) || root > double(t_max)) {
+        root = (-half_b + sqrtd) / a;
+        if (root < double(t_min) || root > double(t_max)) return false;
+    }
+    t_max = float(root);
+    return true;
+}
+
+// triangle::intersect, Moller-Trumbore (include/triangle.hpp:40-61). The slot
+// holds (p0, e1.x) (e1.yz, e2.xy) (e2.z, ...).
+__device__ __forceinline__ bool tri_hit(float4 a, float4 b, float4 c, V o, V d, float t_min, float& t_max,
+                                        float& u_out, float& v_out) {
+    const V p0 = mk(a.x, a.y, a.z), e1 = mk(a.w, b.x, b.y), e2 = mk(b.z, b.w, c.x);
+    const V pvec = cross(d, e2);
+    const float det = dot(e1, pvec);
+    if (fabsf(det) < 1e-12f) return false;
+    const float inv_det = 1.0f / det;
+    const V tvec = o - p0;
+    const float u = dot(tvec, pvec) * inv_det;
+    if (u < 0 || u > 1) return false;
+    const V qvec = cross(tvec, e1);
+    const float v = dot(d, qvec) * inv_det;
+    if (v < 0 || u + v > 1) return false;
+    const float t = dot(e2, qvec) * inv_det;
+    if (t < t_min || t > t_max) return false;
+    t_max = t;
+    u_out = u;
+    v_out = v;
+    return true;
+}
+
+// affine::vector / point (include/transform.hpp:15-20) with rows (m[r][0..2], t[r]).
+__device__ __forceinline__ V aff_vector(const float4 r[3], V v) {
+    return {r[0].x * v.x + r[0].y * v.y + r[0].z * v.z, r[1].x * v.x + r[1].y * v.y + r[1].z * v.z,
+            r[2].x * v.x + r[2].y * v.y + r[2].z * v.z};
+}
+__device__ __forceinline__ V aff_point(const float4 r[3], V p) { return aff_vector(r, p) + mk(r[0].w, r[1].w, r[2].w); }
+// affine::transposed (include/transform.hpp:23-27).
+__device__ __forceinline__ V aff_transposed(const float4 r[3], V v) {
+    return {r[0].x * v.x + r[1].x * v.y + r[2].x * v.z, r[0].y * v.x + r[1].y * v.y + r[2].y * v.z,
+            r[0].z * v.x + r[1].z * v.y + r[2].z * v.z};
+}
+
+// ---- BVH4 traversal (include/bvh.hpp:57-106) ---------------------------------------------
+// Pops an entry; skips it when t >= t_max; a leaf calls leaf(first, count);
+// a node is slab-tested against [t_min, t_max] for its four children, and the
+// children hit are pushed farthest first, equal entry distances in child
+// order (a stable sort by descending t), so the nearest is popped next --
+// the same visiting order as the reference, which decides equal-t ties.
+// Returns false if the stack would overflow (the ray is then abandoned).
+template <bool COUNT, class Leaf>
+__device__ __forceinline__ bool traverse(const float4* __restrict__ nodes, uint32_t root, V o, V d, float t_min,
+                                         float& t_max, StackEntry* stack, int base, Counts& cnt, Leaf&& leaf) {
+    const float ix = 1.0f / d.x, iy = 1.0f / d.y, iz = 1.0f / d.z;
+    int top = base;
+    stack[top++] = {root, 0u, t_min, 0u};
+    while (top > base) {
+        const StackEntry e = stack[--top];
+        if (e.t >= t_max) continue;
+        if (e.count != 0) {
+            if (!leaf(e.first, e.count, top)) return false;
+            continue;
+        }
+        const float4* nd = nodes + 8 * size_t(e.first);
+        const float4 lox = __ldg(nd + 0), loy = __ldg(nd + 1), loz = __ldg(nd + 2);
+        const float4 hix = __ldg(nd + 3), hiy = __ldg(nd + 4), hiz = __ldg(nd + 5);
+        const uint4 first = __ldg(reinterpret_cast<const uint4*>(nd + 6));
+        const uint4 count = __ldg(reinterpret_cast<const uint4*>(nd + 7));
+        if (COUNT) cnt.nodes++;
+        float tn[4];
+        int mask = 0;
+#define PT_SLAB(C, L)                                                                                  \
+    {                                                                                                  \
+        const float x0 = (lox.L - o.x) * ix, x1 = (hix.L - o.x) * ix;                                  \
+        const float y0 = (loy.L - o.y) * iy, y1 = (hiy.L - o.y) * iy;                                  \
+        const float z0 = (loz.L - o.z) * iz, z1 = (hiz.L - o.z) * iz;                                  \
+        const float n_ = sse_max(sse_max(sse_min(x0, x1), sse_min(y0, y1)), sse_max(sse_min(z0, z1), t_min)); \
+        const float f_ = sse_min(sse_min(sse_max(x0, x1), sse_max(y0, y1)), sse_min(sse_max(z0, z1), t_max)); \
+        tn[C] = n_;                                                                                    \
+        mask |= (n_ <= f_) ? (1 << C) : 0;                                                             \
+    }
+        PT_SLAB(0, x)
+        PT_SLAB(1, y)
+        PT_SLAB(2, z)
+        PT_SLAB(3, w)
+#undef PT_SLAB
+        if (mask == 0) continue;
+        const int n = __popc(mask);
+        if (top + n > PT_STACK_MAX) return false;
+        const uint32_t fs[4] = {first.x, first.y, first.z, first.w};
+        const uint32_t cs[4] = {count.x, count.y, count.z, count.w};
+        // Position of child c among the hit children after a stable sort by
+        // descending entry distance: those strictly farther, plus equal ones
+        // with a smaller child number.
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            if (!(mask & (1 << c))) continue;
+            int pos = 0;
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                if (k == c || !(mask & (1 << k))) continue;
+                pos += (tn[k] > tn[c] || (tn[k] == tn[c] && k < c)) ? 1 : 0;
+            }
+            stack[top + pos] = {fs[c], cs[c], tn[c], 0u};
+        }
+        top += n;
+    }
+    return true;
+}
+
+// ---- the scene queries ---------------------------------------------------------------------
+// geometry::hit (include/geometry.hpp:111-152) up to the choice of the
+// nearest primitive: large spheres in double, then the flat tree, then the
+// instance tree whose leaves walk each mesh's tree with the ray moved into
+// object space (hit_instance, :212-229). Returns false on stack overflow.
+template <bool COUNT>
+__device__ __forceinline__ bool closest(const PtSceneDev& S, V o, V d, float t_min, float& t_max, Hit& h,
+                                        StackEntry* stack, Counts& cnt) {
+    h.kind = PT_HIT_NONE;
+    h.index = 0;
+    h.inst = 0;
+    h.u = 0;
+    h.v = 0;
+    for (uint32_t i = 0; i < S.n_large; ++i)
+        if (sphere_hit_double(__ldg(S.large + i), o, d, t_min, t_max)) {
+            h.kind = PT_HIT_LARGE;
+            h.index = i;
+        }
+
+    // One leaf of the flat tree: slots [first, first + count).
+    auto flat_leaf = [&](uint32_t first, uint32_t count_word, int) -> bool {
+        const uint32_t count = count_word & PT_COUNT_MASK;
+        const bool spheres = (count_word & PT_LEAF_HAS_SPHERE) != 0;
+        for (uint32_t k = first; k < first + count; ++k) {
+            const float4* s = S.slots + 3 * size_t(k);
+            if (COUNT) cnt.order++;
+            if (spheres) {
+                const float4 c = __ldg(s + 2);
+                if (fbits(c.y) & PT_SLOT_SPHERE) {
+                    if (COUNT) cnt.spheres++;
+                    if (sphere_hit(__ldg(s), o, d, t_min, t_max)) {
+                        h.kind = PT_HIT_SPHERE;
+                        h.index = k;
+                    }
+                    continue;
+                }
+                if (COUNT) cnt.tris++;
+                if (tri_hit(__ldg(s), __ldg(s + 1), c, o, d, t_min, t_max, h.u, h.v)) {
+                    h.kind = PT_HIT_TRIANGLE;
+                    h.index = k;
+                }
+            } else {
+                if (COUNT) cnt.tris++;
+                if (tri_hit(__ldg(s), __ldg(s + 1), __ldg(s + 2), o, d, t_min, t_max, h.u, h.v)) {
+                    h.kind = PT_HIT_TRIANGLE;
+                    h.index = k;
+                }
+            }
+        }
+        return true;
+    };
+
+    // One leaf of the instance tree: each instance walks its mesh's tree on
+    // the stack above the current top.
+    auto inst_leaf = [&](uint32_t first, uint32_t count_word, int top) -> bool {
+        const uint32_t count = count_word & PT_COUNT_MASK;
+        for (uint32_t k = first; k < first + count; ++k) {
+            const float4* is = S.islots + 4 * size_t(k);
+            float4 rows[3] = {__ldg(is), __ldg(is + 1), __ldg(is + 2)};
+            const uint4 meta = __ldg(reinterpret_cast<const uint4*>(is + 3));
+            if (COUNT) { cnt.order++; cnt.insts++; }
+            const V lo = aff_point(rows, o), ld = aff_vector(rows, d);
+            bool found = false;
+            uint32_t slot = 0;
+            float u = h.u, v = h.v;
+            auto mesh_leaf = [&](uint32_t f, uint32_t cw, int) -> bool {
+                const uint32_t c = cw & PT_COUNT_MASK;
+                for (uint32_t q = f; q < f + c; ++q) {
+                    const float4* s = S.slots + 3 * size_t(q);
+                    if (COUNT) { cnt.order++; cnt.tris++; }
+                    if (tri_hit(__ldg(s), __ldg(s + 1), __ldg(s + 2), lo, ld, t_min, t_max, u, v)) {
+                        found = true;
+                        slot = q;
+                    }
+                }
+                return true;
+            };
+            if (!traverse<COUNT>(S.nodes, meta.x, lo, ld, t_min, t_max, stack, top, cnt, mesh_leaf)) return false;
+            if (found) {
+                h.kind = PT_HIT_INSTANCE;
+                h.index = slot;
+                h.inst = meta.y;
+                h.u = u;
+                h.v = v;
+            }
+        }
+        return true;
+    };
+
+    if (S.use_bvh) {
+        if (S.flat_root != PT_NONE)
+            if (!traverse<COUNT>(S.nodes, S.flat_root, o, d, t_min, t_max, stack, 0, cnt, flat_leaf)) return false;
+        if (S.inst_root != PT_NONE)
+            if (!traverse<COUNT>(S.nodes, S.inst_root, o, d, t_min, t_max, stack, 0, cnt, inst_leaf)) return false;
+    } else {
+        // Without the BVH every primitive, then every instance, in order (:135-139).
+        if (S.n_flat_slots) flat_leaf(0, S.n_flat_slots | PT_LEAF_HAS_SPHERE, 0);
+        if (S.n_instances)
+            if (!inst_leaf(0, S.n_instances, 0)) return false;
+    }
+    return true;
+}
+
+// geometry::occluded (include/geometry.hpp:156-190): whether anything lies on
+// the ray within [t_min, t_max]. Stops at the first blocker, which is where
+// the reference's traversal stops doing work too (it collapses t_far to t_min).
+// *overflow is set when a stack would overflow.
+template <bool COUNT>
+__device__ __forceinline__ bool occluded(const PtSceneDev& S, V o, V d, float t_min, float t_max,
+                                         StackEntry* stack, Counts& cnt, bool* overflow) {
+    for (uint32_t i = 0; i < S.n_large; ++i) {
+        float t = t_max;
+        if (sphere_hit_double(__ldg(S.large + i), o, d, t_min, t)) return true;
+    }
+    bool blocked = false;
+    float t_far = t_max;
+    auto flat_leaf = [&](uint32_t first, uint32_t count_word, int) -> bool {
+        const uint32_t count = count_word & PT_COUNT_MASK;
+        const bool spheres = (count_word & PT_LEAF_HAS_SPHERE) != 0;
+        for (uint32_t k = first; k < first + count && !blocked; ++k) {
+            const float4* s = S.slots + 3 * size_t(k);
+            float t = t_far, u, v;
+            if (COUNT) cnt.order++;
+            const float4 c = __ldg(s + 2);
+            if (spheres && (fbits(c.y) & PT_SLOT_SPHERE)) {
+                if (COUNT) cnt.spheres++;
+                blocked = sphere_hit(__ldg(s), o, d, t_min, t);
+            } else {
+                if (COUNT) cnt.tris++;
+                blocked = tri_hit(__ldg(s), __ldg(s + 1), c, o, d, t_min, t, u, v);
+            }
+        }
+        if (blocked) t_far = t_min;
+        return true;
+    };
+    auto inst_leaf = [&](uint32_t first, uint32_t count_word, int top) -> bool {
+        const uint32_t count = count_word & PT_COUNT_MASK;
+        for (uint32_t k = first; k < first + count && !blocked; ++k) {
+            const float4* is = S.islots + 4 * size_t(k);
+            float4 rows[3] = {__ldg(is), __ldg(is + 1), __ldg(is + 2)};
+            const uint4 meta = __ldg(reinterpret_cast<const uint4*>(is + 3));
+            if (COUNT) { cnt.order++; cnt.insts++; }
+            const V lo = aff_point(rows, o), ld = aff_vector(rows, d);
+            float t_mesh = t_far;
+            bool found = false;
+            auto mesh_leaf = [&](uint32_t f, uint32_t cw, int) -> bool {
+                const uint32_t c = cw & PT_COUNT_MASK;
+                for (uint32_t q = f; q < f + c && !found; ++q) {
+                    const float4* s = S.slots + 3 * size_t(q);
+                    float u, v;
+                    if (COUNT) { cnt.order++; cnt.tris++; }
+                    if (tri_hit(__ldg(s), __ldg(s + 1), __ldg(s + 2), lo, ld, t_min, t_mesh, u, v)) {
+                        found = true;
+                        t_mesh = t_min;
+                    }
+                }
+                return true;
+            };
+            if (!traverse<COUNT>(S.nodes, meta.x, lo, ld, t_min, t_mesh, stack, top, cnt, mesh_leaf)) return false;
+            blocked = found;
+        }
+        if (blocked) t_far = t_min;
+        return true;
+    };
+    if (S.use_bvh) {
+        if (S.flat_root != PT_NONE)
+            if (!traverse<COUNT>(S.nodes, S.flat_root, o, d, t_min, t_far, stack, 0, cnt, flat_leaf)) {
+                *overflow = true;
+                return false;
+            }
+        if (!blocked && S.inst_root != PT_NONE) {
+            t_far = t_max;
+            if (!traverse<COUNT>(S.nodes, S.inst_root, o, d, t_min, t_far, stack, 0, cnt, inst_leaf)) {
+                *overflow = true;
+                return false;
+            }
+        }
+    } else {
+        if (S.n_flat_slots) flat_leaf(0, S.n_flat_slots | PT_LEAF_HAS_SPHERE, 0);
+        if (!blocked && S.n_instances) {
+            t_far = t_max;
+            if (!inst_leaf(0, S.n_instances, 0)) {
+                *overflow = true;
+                return false;
+            }
+        }
+    }
+    return blocked;
+}
+
+// The original primitive number of a closest hit (for ray queries).
+__device__ __forceinline__ void resolve(const PtSceneDev& S, const Hit& h, uint32_t& index, uint32_t& sub) {
+    index = h.index;
+    sub = 0;
+    if (h.kind == PT_HIT_SPHERE || h.kind == PT_HIT_TRIANGLE) {
+        index = fbits(__ldg(S.slots + 3 * size_t(h.index) + 2).y) & ~PT_SLOT_SPHERE;
+    } else if (h.kind == PT_HIT_INSTANCE) {
+        index = h.inst;
+        sub = fbits(__ldg(S.slots + 3 * size_t(h.index) + 2).y);
+    }
+}
+
+// ---- hit records (include/hittable.hpp:7-21) -------------------------------------------------
+struct Rec {
+    V p, normal;
+    float t;
+    bool front_face;
+    bool sampled_light;
+    uint32_t mat;
+};
+
+// sphere::fill (include/sphere.hpp:50-58)
+__device__ __forceinline__ void fill_sphere(float4 cr, uint32_t mat, V o, V d, float t, Rec& rec) {
+    rec.t = t;
+    rec.p = o + d * t;
+    const V outward = (rec.p - xyz(cr)) * (1.0f / cr.w);
+    rec.front_face = dot(d, outward) < 0;
+    rec.normal = rec.front_face ? outward : -outward;
+    rec.mat = mat;
+}
+
+// triangle::fill (include/triangle.hpp:63-74), direction d in the triangle's space.
+__device__ __forceinline__ void fill_triangle(const PtShadeTri* __restrict__ tri, uint32_t g, V d, float u, float v,
+                                              Rec& rec) {
+    const float4 a = __ldg(&tri[g].n0_mat), b = __ldg(&tri[g].n1), c = __ldg(&tri[g].n2), f = __ldg(&tri[g].fn);
+    rec.front_face = dot(d, xyz(f)) < 0;
+    const float w = 1 - u - v;
+    const V n = normalize(xyz(a) * w + xyz(b) * u + xyz(c) * v);
+    rec.normal = rec.front_face ? n : -n;
+    rec.mat = fbits(a.w);
+}
+
+// The record geometry::hit fills for the nearest primitive (:141-151,
+// fill_instance :234-244).
+__device__ __forceinline__ void fill(const PtSceneDev& S, const Hit& h, V o, V d, float t, Rec& rec) {
+    rec.sampled_light = false;
+    rec.t = t;
+    switch (h.kind) {
+        case PT_HIT_LARGE:
+            fill_sphere(__ldg(S.large + h.index), __ldg(S.large_mat + h.index), o, d, t, rec);
+            break;
+        case PT_HIT_SPHERE: {
+            const uint32_t i = fbits(__ldg(S.slots + 3 * size_t(h.index) + 2).y) & ~PT_SLOT_SPHERE;
+            const float4 cr = __ldg(&S.sph[i].cr);
+            const uint32_t m = __ldg(&S.sph[i].mat);
+            fill_sphere(cr, m, o, d, t, rec);
+            rec.sampled_light = S.sample_lights && (fbits(__ldg(&S.mat[m].ior_flags.y)) & PT_MF_EMITS) != 0;
+            break;
+        }
+        case PT_HIT_TRIANGLE: {
+            const uint32_t i = fbits(__ldg(S.slots + 3 * size_t(h.index) + 2).y);
+            rec.p = o + d * t;
+            fill_triangle(S.tri, i, d, h.u, h.v, rec);
+            break;
+        }
+        case PT_HIT_INSTANCE: {
+            const PtShadeInst* in = S.inst + h.inst;
+            float4 rows[3] = {__ldg(&in->row[0]), __ldg(&in->row[1]), __ldg(&in->row[2])};
+            const uint32_t tri_base = __ldg(&in->tri_base), over = __ldg(&in->material);
+            const uint32_t sub = fbits(__ldg(S.slots + 3 * size_t(h.index) + 2).y);
+            const V ld = aff_vector(rows, d);
+            fill_triangle(S.tri, tri_base + sub, ld, h.u, h.v, rec);
+            rec.p = o + d * t;
+            rec.normal = normalize(aff_transposed(rows, rec.normal));
+            if (over != PT_NONE) rec.mat = over;
+            break;
+        }
+        default:
+            break;
+    }
+}
+
+// ---- random numbers (include/vec3.hpp:11-52) ------------------------------------------------
+struct Rng {
+    uint64_t s0, s1, s2, s3;
+    // xoshiro256p::seed: splitmix64 across the four words.
+    __device__ __forceinline__ void seed(uint64_t seed) {
+        uint64_t* w[4] = {&s0, &s1, &s2, &s3};
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            uint64_t z = (seed += 0x9e3779b97f4a7c15ull);
+            z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+            z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+            *w[k] = z ^ (z >> 31);
+        }
+    }
+    __device__ __forceinline__ uint64_t next() {
+        const uint64_t result = s0 + s3, t = s1 << 17;
+        s2 ^= s0;
+        s3 ^= s1;
+        s1 ^= s2;
+        s0 ^= s3;
+        s2 ^= t;
+        s3 = (s3 << 45) | (s3 >> 19);
+        return result;
+    }
+    // random_real: the top 24 bits as a float in [0, 1).
+    __device__ __forceinline__ float real() { return float(next() >> 40) * 0x1.0p-24f; }
+};
+
+// The per-(pixel, sample) stream of PT_RNG_SAMPLE: splitmix64's finaliser
+// over (seed, row, column), then the sample number, seeds xoshiro256+.
+__device__ __host__ __forceinline__ uint64_t sample_stream_seed(uint64_t seed, int i, int j, uint32_t s) {
+    uint64_t x = seed ^ ((uint64_t(uint32_t(j)) << 32) | uint32_t(i));
+    x = (x ^ (x >> 30)) * 0xbf58476d1ce4e5b9ull;
+    x = (x ^ (x >> 27)) * 0x94d049bb133111ebull;
+    x ^= x >> 31;
+    return x ^ (uint64_t(s) * 0xd6e8feb86659fd93ull);
+}
+
+// ---- the Sobol sampler (include/sampler.hpp:35-127) -----------------------------------------
+__device__ __forceinline__ uint32_t hash_u32(uint32_t x) {
+    x ^= x >> 16;
+    x *= 0x7feb352du;
+    x ^= x >> 15;
+    x *= 0x846ca68bu;
+    x ^= x >> 16;
+    return x;
+}
+__device__ __forceinline__ uint32_t lk_permute(uint32_t x, uint32_t seed) {
+    x += seed;
+    x ^= x * 0x6c50b47cu;
+    x ^= x * 0xb82f1e52u;
+    x ^= x * 0xc7afe638u;
+    x ^= x * 0x8d22f6e6u;
+    return x;
+}
+// The second Sobol dimension, bit-reversed (sobol_1_reversed, sampler.hpp:91-94).
+// Its direction numbers are Pascal's triangle mod 2, so bit m of the result
+// is the parity of the set bits k of i with k a bitwise superset of m (Lucas'
+// theorem): a superset-XOR transform over the 5-bit positions, five shift-and-
+// mask steps instead of four table lookups.
+__device__ __forceinline__ uint32_t sobol_1_reversed(uint32_t r) {
+    r ^= (r >> 1) & 0x55555555u;
+    r ^= (r >> 2) & 0x33333333u;
+    r ^= (r >> 4) & 0x0f0f0f0fu;
+    r ^= (r >> 8) & 0x00ff00ffu;
+    r ^= (r >> 16) & 0x0000ffffu;
+    return r;
+}
+
+struct Sampler {
+    uint32_t pixel_seed, index;
+    int base;
+    // begin_sample (sampler.hpp:98-104)
+    __device__ __forceinline__ void begin(uint64_t seed, int i, int j, uint32_t idx) {
+        pixel_seed = hash_u32(uint32_t(i) * 0x9e3779b1u ^
+                              hash_u32(uint32_t(j) ^ hash_u32(uint32_t(seed) ^ uint32_t(seed >> 32))));
+        index = idx;
+        base = 0;
+    }
+    // set_bounce (sampler.hpp:127)
+    __device__ __forceinline__ void set_bounce(int k) { base = 1 + 2 * k; }
+    // sample_2d (sampler.hpp:107-124): QMC for pairs 0..4, the random stream after.
+    __device__ __forceinline__ void sample_2d(int pair_offset, Rng& rng, float& a, float& b) const {
+        const int pair = base + pair_offset;
+        if (pair > 4) {
+            a = rng.real();
+            b = rng.real();
+            return;
+        }
+        const uint32_t seed = hash_u32(pixel_seed + uint32_t(pair) * 0x68bc21ebu);
+        const uint32_t i = __brev(lk_permute(__brev(index), seed));
+        const uint32_t x = __brev(lk_permute(i, seed ^ 0xa511e9b3u));
+        const uint32_t y = __brev(lk_permute(sobol_1_reversed(i), seed ^ 0x63d83595u));
+        a = float(x >> 8) * 0x1.0p-24f;
+        b = float(y >> 8) * 0x1.0p-24f;
+    }
+};
+
+// ---- materials (include/material.hpp) ----------------------------------------------------------
+__device__ __forceinline__ V reflect(V v, V n) { return v - n * (2 * dot(v, n)); }
+__device__ __forceinline__ V refract(V uv, V n, float ratio) {
+    const float cos_theta = fminf(dot(-uv, n), 1.0f);
+    const V r_perp = (uv + n * cos_theta) * ratio;
+    const V r_parallel = n * -sqrtf(fabsf(1 - dot(r_perp, r_perp)));
+    return r_perp + r_parallel;
+}
+// random_in_unit_sphere (vec3.hpp:121-127). vec3::random(-1, 1) builds the
+// vector from three calls in one constructor argument list, which GCC on
+// x86-64 evaluates right to left: z is drawn first, x last. The rejection
+// loop is bounded: 64 misses in a row has probability 0.48^64 (~1e-20) for a
+// real stream, but an all-zero xoshiro state (which a caller could supply
+// as a snapshot) repeats (-1,-1,-1) forever; the bound turns that into a
+// zero offset instead of a hung kernel.
+__device__ __forceinline__ V random_in_unit_sphere(Rng& rng) {
+    for (int tries = 0; tries < 64; ++tries) {
+        const float z = -1.0f + 2.0f * rng.real();
+        const float y = -1.0f + 2.0f * rng.real();
+        const float x = -1.0f + 2.0f * rng.real();
+        const V p = mk(x, y, z);
+        if (dot(p, p) >= 1) continue;
+        return p;
+    }
+    return mk(0, 0, 0);
+}
+
+// material::scatter for the four kinds: lambertian :59-74, metal :85-91,
+// diffuse_light :97-102, dielectric :113-136.
+__device__ __forceinline__ bool scatter(const PtMaterial& m, uint32_t type, V d_in, const Rec& rec,
+                                        const Sampler& smp, Rng& rng, V& attenuation, V& dir) {
+    if (type == PT_MAT_LAMBERTIAN) {
+        float a, b;
+        smp.sample_2d(0, rng, a, b);
+        const float r = sqrtf(a), phi = 2 * float(M_PI) * b;
+        const V n = rec.normal;
+        const float sign = copysignf(1.0f, n.z);
+        const float p = -1 / (sign + n.z), q = n.x * n.y * p;
+        const V t1 = mk(1 + sign * n.x * n.x * p, sign * q, -sign * n.x);
+        const V t2 = mk(q, sign + n.y * n.y * p, -n.y);
+        dir = t1 * (r * cosf(phi)) + t2 * (r * sinf(phi)) + n * sqrtf(fmaxf(0.0f, 1 - a));
+        attenuation = xyz(m.albedo_type);
+        return true;
+    }
+    if (type == PT_MAT_METAL) {
+        const V reflected = reflect(normalize(d_in), rec.normal);
+        dir = reflected + random_in_unit_sphere(rng) * m.emission_fuzz.w;
+        attenuation = xyz(m.albedo_type);
+        return dot(dir, rec.normal) > 0;
+    }
+    if (type == PT_MAT_DIELECTRIC) {
+        attenuation = mk(1, 1, 1);
+        const float ior = m.ior_flags.x;
+        const float ratio = rec.front_face ? (1 / ior) : ior;
+        const V unit = normalize(d_in);
+        const float cos_theta = fminf(dot(-unit, rec.normal), 1.0f);
+        const float sin_theta = sqrtf(1 - cos_theta * cos_theta);
+        const bool cannot_refract = ratio * sin_theta > 1;
+        bool refl = cannot_refract;
+        if (!refl) {
+            // schlick (:131-136)
+            float r0 = (1 - ratio) / (1 + ratio);
+            r0 = r0 * r0;
+            const float x = 1 - cos_theta, x2 = x * x;
+            const float sch = r0 + (1 - r0) * x2 * x2 * x;
+            refl = sch > rng.real();
+        }
+        dir = refl ? reflect(unit, rec.normal) : refract(unit, rec.normal, ratio);
+        return true;
+    }
+    return false;  // diffuse_light
+}
+
+}  // namespace ptd

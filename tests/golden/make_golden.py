@@ -1,0 +1,113 @@
+"""Writes the golden fixtures under tests/golden/ from the reference itself.
+
+Run in a checkout that has the reference (PT_REFERENCE_DIR, default
+/root/reference) with oracle/_ref built (python oracle/build.py). The
+fixtures let the tests pin the CPU restatement on machines without the
+reference:
+
+* reference_blocks.npz -- the reference's own statistical render fixture
+  (tests/reference.json: per-20x20-block mean linear colour and sigma over 16
+  seeds, 960x540 at 200 spp) for the scenes this path renders: materials,
+  field, room;
+* ref_hits_*.npz      -- rays and the reference's closest/any hits on them;
+* ref_render_*.npz    -- small renders by the reference's own per-row stream,
+  with the xoshiro state captured before every sample's path;
+* ref_trees.json      -- digests of the trees the reference's geometry::build
+  makes for every scene generator.
+
+    python tests/golden/make_golden.py
+"""
+from __future__ import annotations
+
+import hashlib
+import json
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+import photon_tracer_b200 as pt  # noqa: E402
+from photon_tracer_b200 import abi  # noqa: E402
+from oracle.oracle import Reference, reference_trees  # noqa: E402
+
+REFERENCE = os.environ.get("PT_REFERENCE_DIR", "/root/reference")
+
+# (name, generator kind, param, ray box) of the hit fixtures
+HIT_CASES = [
+    ("room_mesh", abi.PT_GEN_ROOM_MESH, 6, ([-1, -1, -1], [1, 1, 1]), 8192),
+    ("random_spheres", abi.PT_GEN_RANDOM_SPHERES, 0, ([-12, 0, -12], [12, 3, 12]), 8192),
+    ("ref_room", abi.PT_GEN_REF_ROOM, 0, ([-1.75, -1, -3.5], [1.75, 1, 0.5]), 4096),
+    ("instances", abi.PT_GEN_INSTANCES, 400, ([-30, 0, -30], [30, 6, 30]), 4096),
+]
+RENDER_CASES = [
+    ("room_mesh", abi.PT_GEN_ROOM_MESH, 6, 32, 32, 2),
+    ("random_spheres", abi.PT_GEN_RANDOM_SPHERES, 0, 40, 23, 2),
+    ("ref_field", abi.PT_GEN_REF_FIELD, 0, 40, 23, 2),
+    ("instances", abi.PT_GEN_INSTANCES, 400, 32, 18, 1),
+]
+TREE_CASES = [("ref_materials", abi.PT_GEN_REF_MATERIALS, 0), ("ref_field", abi.PT_GEN_REF_FIELD, 0),
+              ("ref_room", abi.PT_GEN_REF_ROOM, 0), ("random_spheres", abi.PT_GEN_RANDOM_SPHERES, 0),
+              ("room_mesh", abi.PT_GEN_ROOM_MESH, 6), ("instances", abi.PT_GEN_INSTANCES, 0)]
+
+
+def tree_digest(trees) -> list:
+    out = []
+    for t in trees.arrays:
+        if t is None:
+            out.append(None)
+        else:
+            h = hashlib.sha256(t[0].tobytes() + t[1].tobytes()).hexdigest()
+            out.append([int(len(t[0])), int(len(t[1])), h])
+    return out
+
+
+def main():
+    ref_json = os.path.join(REFERENCE, "tests", "reference.json")
+    with open(ref_json) as f:
+        ref = json.load(f)
+    blocks = {"width": ref["width"], "spp": ref["spp"], "block": ref["block"], "seeds": ref["seeds"]}
+    arrays = {}
+    for scene in ("materials", "field", "room"):
+        s = ref["scenes"][scene]
+        arrays[f"{scene}_blocks"] = np.array(s["blocks"], np.int32)
+        arrays[f"{scene}_mean"] = np.array(s["mean"], np.float64)
+        arrays[f"{scene}_sigma"] = np.array(s["sigma"], np.float64)
+    np.savez_compressed(os.path.join(HERE, "reference_blocks.npz"), meta=json.dumps(blocks), **arrays)
+
+    for name, kind, param, (lo, hi), n in HIT_CASES:
+        g = pt.Generated(kind, seed=1, param=param)
+        r = Reference(g.desc)
+        rays = pt.generate_rays(2024, lo, hi, n)
+        # a few axis-aligned rays: zero direction components give infinite
+        # inverses in the slab test
+        rays[:6, 3:] = np.array([[1, 0, 0], [0, 1, 0], [0, 0, 1], [-1, 0, 0], [0, -1, 0], [0, 0, -1]], np.float32)
+        hits, bad = r.trace_closest(rays)
+        assert bad == 0, "re-composed hit disagrees with geometry::hit"
+        occ = r.trace_any(rays)
+        np.savez_compressed(os.path.join(HERE, f"ref_hits_{name}.npz"), rays=rays, hits=hits.view(np.uint32).reshape(-1, 6),
+                            occluded=occ, kind=kind, param=param)
+
+    for name, kind, param, w, h, spp in RENDER_CASES:
+        g = pt.Generated(kind, seed=1, param=param)
+        r = Reference(g.desc)
+        img, aux, rays, states = r.render_snapshot(g.camera, w, h, spp, 10, seed=5)
+        cam = np.frombuffer(bytes(g.camera), np.float32)
+        np.savez_compressed(os.path.join(HERE, f"ref_render_{name}.npz"), image=img, aux=aux, rays=np.uint64(rays),
+                            states=states, camera=cam, kind=kind, param=param, width=w, height=h, spp=spp, seed=5)
+
+    digests = {}
+    for name, kind, param in TREE_CASES:
+        g = pt.Generated(kind, seed=1, param=param)
+        r = Reference(g.desc)
+        digests[name] = {"kind": kind, "param": param, "trees": tree_digest(reference_trees(r, g.desc))}
+    with open(os.path.join(HERE, "ref_trees.json"), "w") as f:
+        json.dump(digests, f, indent=1)
+    print("wrote fixtures to", HERE)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,187 @@
+"""Ray queries on the GPU through the C ABI, against the oracle: closest hits
+(kind, primitive, sub-triangle, t, u, v) must be bit-identical, any-hit
+answers identical, traversal work counters identical."""
+import os
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN, golden
+
+pytestmark = pytest.mark.gpu
+
+HIT_FIXTURES = sorted(f for f in os.listdir(GOLDEN) if f.startswith("ref_hits_"))
+
+
+@pytest.fixture(scope="module")
+def pt(built):
+    import torch
+    assert torch.cuda.is_available(), "GPU tests need a CUDA device"
+    return built
+
+
+def assert_hits_equal(got, want, rays=None):
+    if got.tobytes() == want.tobytes():
+        return
+    bad = np.nonzero(got.view(np.uint32).reshape(-1, 6) != want.view(np.uint32).reshape(-1, 6))[0]
+    i = int(bad[0])
+    msg = f"{len(np.unique(bad))} rays differ; first ray {i}: got {got[i]} want {want[i]}"
+    if rays is not None:
+        msg += f" ray {rays[i]}"
+    raise AssertionError(msg)
+
+
+@pytest.mark.parametrize("name", HIT_FIXTURES)
+def test_hits_match_reference_fixture(pt, name):
+    f = golden(name)
+    g = pt.Generated(int(f["kind"]), seed=1, param=int(f["param"]))
+    s = pt.Scene(g)
+    hits = s.trace_closest(f["rays"])
+    assert_hits_equal(hits, f["hits"].reshape(-1).view(hits.dtype), f["rays"])
+    assert np.array_equal(s.trace_any(f["rays"]), f["occluded"])
+
+
+def test_room_mesh_ray_set_bit_exact(pt):
+    """The 81,920-triangle room scene and the seeded ray-query set (origins in
+    the room, directions uniform on the sphere): the first 1M rays against
+    the oracle, bit for bit, and the traversal counters equal."""
+    from oracle.oracle import Oracle
+    from photon_tracer_b200 import abi
+    g = pt.Generated(abi.PT_GEN_ROOM_MESH, seed=1)
+    s = pt.Scene(g)
+    o = Oracle(g.desc)
+    rays = pt.generate_rays(1, [-1, -1, -1], [1, 1, 1], 1 << 20)
+    assert_hits_equal(s.trace_closest(rays), o.trace_closest(rays), rays)
+    sub = rays[:200000]
+    _, counts = o.trace_closest(sub, counts=True)
+    assert np.array_equal(s.trace_count(sub), counts)
+    occ_gpu = s.trace_any(rays, 0.001, 0.5)
+    assert np.array_equal(occ_gpu, o.trace_any(rays, 0.001, 0.5))
+
+
+def test_full_ray_set_consistency(pt):
+    """All 16,777,216 rays of the query set: GPU closest hits on a strided
+    subset equal the oracle's, and the full set is deterministic."""
+    from oracle.oracle import Oracle
+    from photon_tracer_b200 import abi
+    g = pt.Generated(abi.PT_GEN_ROOM_MESH, seed=1)
+    s = pt.Scene(g)
+    rays = pt.generate_rays(1, [-1, -1, -1], [1, 1, 1], 1 << 24)
+    h1 = s.trace_closest(rays)
+    h2 = s.trace_closest(rays)
+    assert h1.tobytes() == h2.tobytes()
+    idx = np.arange(0, len(rays), 97)
+    assert_hits_equal(h1[idx], Oracle(g.desc).trace_closest(rays[idx]), rays[idx])
+    # inside a closed room (open front) most rays hit something
+    assert (h1["kind"] != abi.PT_HIT_NONE).mean() > 0.8
+
+
+@pytest.mark.parametrize("kind,param,box", [
+    ("RANDOM_SPHERES", 0, ([-12, 0, -12], [12, 3, 12])),
+    ("INSTANCES", 0, ([-100, 0, -100], [100, 8, 100])),
+    ("REF_FIELD", 0, ([-3, -0.5, -3], [3, 1.5, 0])),
+    ("BATCH_SCENE", 0, ([-2, -2, -2], [2, 2, 2])),
+])
+def test_generators_bit_exact(pt, kind, param, box):
+    from oracle.oracle import Oracle
+    from photon_tracer_b200 import abi
+    g = pt.Generated(getattr(abi, "PT_GEN_" + kind), seed=5, param=param)
+    s = pt.Scene(g)
+    o = Oracle(g.desc)
+    rays = pt.generate_rays(11, box[0], box[1], 100000)
+    assert_hits_equal(s.trace_closest(rays), o.trace_closest(rays), rays)
+    assert np.array_equal(s.trace_any(rays), o.trace_any(rays))
+    _, counts = o.trace_closest(rays[:20000], counts=True)
+    assert np.array_equal(s.trace_count(rays[:20000]), counts)
+
+
+def test_no_bvh_mode(pt):
+    """geometry::build(false): every primitive tested in order (materials default)."""
+    from oracle.oracle import Oracle
+    from photon_tracer_b200 import abi
+    for gen in (abi.PT_GEN_REF_MATERIALS, abi.PT_GEN_REF_FIELD):
+        g = pt.Generated(gen, seed=1, use_bvh=0)
+        s = pt.Scene(g)
+        rays = pt.generate_rays(2, [-2, -0.5, -2], [2, 1, 0.5], 50000)
+        assert_hits_equal(s.trace_closest(rays), Oracle(g.desc).trace_closest(rays), rays)
+
+
+def _scene_from(pt, materials, spheres=(), tris=(), large=(), use_bvh=1):
+    """A small hand-made description (kept alive on the returned object)."""
+    import ctypes as C
+    from photon_tracer_b200 import abi
+
+    class Desc:
+        pass
+    d = Desc()
+    d.mats = (abi.pt_material * max(1, len(materials)))(*materials)
+    d.sph = (abi.pt_sphere * max(1, len(spheres)))(*spheres)
+    d.lg = (abi.pt_sphere * max(1, len(large)))(*large)
+    d.tri = (abi.pt_triangle * max(1, len(tris)))(*tris)
+    d.desc = abi.pt_scene_desc(materials=d.mats, n_materials=len(materials), spheres=d.sph, n_spheres=len(spheres),
+                               large_spheres=d.lg, n_large_spheres=len(large), triangles=d.tri, n_triangles=len(tris),
+                               use_bvh=use_bvh, sky=1, sample_lights=1)
+    d.desc_ptr = C.pointer(d.desc)
+    return d
+
+
+def _tri(pt, a, b, c, mat=0):
+    from photon_tracer_b200 import abi
+    a, b, c = (np.array(x, np.float32) for x in (a, b, c))
+    e1, e2 = b - a, c - a
+    n = np.cross(e1.astype(np.float64), e2.astype(np.float64))
+    n = (n / np.linalg.norm(n)).astype(np.float32)
+    t = abi.pt_triangle(material=mat)
+    for name, v in [("p0", a), ("e1", e1), ("e2", e2), ("n0", n), ("n1", n), ("n2", n), ("face_normal", n),
+                    ("p1", b), ("p2", c)]:
+        setattr(t, name, abi.F3(*v.tolist()))
+    return t
+
+
+def test_edge_cases_ties_empty_degenerate(pt):
+    """Equal-t ties (duplicate and coplanar triangles, concentric spheres),
+    degenerate triangles, an empty scene, axis-aligned and zero directions."""
+    from oracle.oracle import Oracle
+    from photon_tracer_b200 import abi
+    m = [abi.pt_material(type=0, albedo=abi.F3(0.5, 0.5, 0.5))]
+    tris = []
+    for k in range(12):  # a stack of duplicates at z = 0 and z = -1, plus slivers
+        tris.append(_tri(pt, (-1, -1, 0), (1, -1, 0), (0, 1, 0)))
+        tris.append(_tri(pt, (-1, -1, -1), (1, -1, -1), (1, 1, -1)))
+    tris.append(_tri(pt, (0, 0, 0.5), (1, 0, 0.5), (2, 0, 0.5)))  # zero area
+    sph = [abi.pt_sphere(center=abi.F3(0, 0, -2), radius=0.5), abi.pt_sphere(center=abi.F3(0, 0, -2), radius=0.5),
+           abi.pt_sphere(center=abi.F3(0, 0, -2), radius=-0.3)]
+    lg = [abi.pt_sphere(center=abi.F3(0, -1001, 0), radius=1000.0)]
+    rng = np.random.default_rng(3)
+    rays = np.concatenate([
+        np.concatenate([rng.uniform(-1, 1, (3000, 2)), np.full((3000, 1), 3), rng.normal(0, 0.2, (3000, 2)),
+                        np.full((3000, 1), -1)], axis=1),
+        np.array([[0, 0, 3, 0, 0, -1], [0.2, -0.3, 3, 0, 0, -1], [0, 0, 3, 0, 0, 0], [0, 0, 0, 1, 0, 0],
+                  [0.5, 0, 0.5, -1, 0, 0], [0, 5, -2, 0, -1, 0], [0, 0, 3, 0, 0, -0.0]]),
+    ]).astype(np.float32)
+    for use_bvh in (1, 0):
+        d = _scene_from(pt, m, sph, tris, lg, use_bvh)
+        s = pt.Scene(d.desc_ptr)
+        o = Oracle(d.desc)
+        assert_hits_equal(s.trace_closest(rays), o.trace_closest(rays), rays)
+        assert np.array_equal(s.trace_any(rays), o.trace_any(rays))
+    empty = _scene_from(pt, m)
+    s = pt.Scene(empty.desc_ptr)
+    h = s.trace_closest(rays)
+    assert np.all(h["kind"] == abi.PT_HIT_NONE) and not s.trace_any(rays).any()
+
+
+def test_device_buffers_entry_point(pt):
+    """pt_trace_closest_device on torch tensors equals the host-buffer call."""
+    import torch
+    from photon_tracer_b200 import abi
+    g = pt.Generated(abi.PT_GEN_ROOM_MESH, seed=1, param=4)
+    s = pt.Scene(g)
+    rays = pt.generate_rays(9, [-1, -1, -1], [1, 1, 1], 65536)
+    d_rays = torch.from_numpy(rays).cuda()
+    d_hits = torch.empty((len(rays), 6), dtype=torch.int32, device="cuda")
+    stream = torch.cuda.current_stream().cuda_stream
+    s.trace_closest_device(d_rays.data_ptr(), len(rays), d_hits.data_ptr(), stream=stream)
+    s.sync(stream)
+    got = d_hits.cpu().numpy().view(abi.HIT_DTYPE).reshape(-1)
+    assert_hits_equal(got, s.trace_closest(rays), rays)

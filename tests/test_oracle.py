@@ -1,0 +1,189 @@
+"""Pins the CPU oracle (the C restatement) before anything is checked against
+it: against the reference's golden vectors committed under tests/golden/,
+against the reference itself (oracle/_ref) where it was built, and against
+the reference's own statistical fixture. Also checks that the scene
+generators reproduce the reference's scenes and constructors. CPU only."""
+import os
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN, golden
+
+HIT_FIXTURES = sorted(f for f in os.listdir(GOLDEN) if f.startswith("ref_hits_"))
+RENDER_FIXTURES = sorted(f for f in os.listdir(GOLDEN) if f.startswith("ref_render_"))
+
+
+def camera_from(arr):
+    from photon_tracer_b200 import abi
+    return abi.pt_camera.from_buffer_copy(np.ascontiguousarray(arr, np.float32).tobytes())
+
+
+@pytest.mark.parametrize("name", HIT_FIXTURES)
+def test_oracle_hits_match_reference_fixture(built, name):
+    from oracle.oracle import Oracle
+    f = golden(name)
+    g = built.Generated(int(f["kind"]), seed=1, param=int(f["param"]))
+    o = Oracle(g.desc)
+    hits = o.trace_closest(f["rays"])
+    assert np.array_equal(hits.view(np.uint32).reshape(-1, 6), f["hits"])
+    assert np.array_equal(o.trace_any(f["rays"]), f["occluded"])
+
+
+@pytest.mark.parametrize("name", RENDER_FIXTURES)
+def test_oracle_renders_match_reference_fixture(built, name):
+    """Per-row stream and snapshot mode both reproduce the reference's floats."""
+    from oracle.oracle import Oracle
+    f = golden(name)
+    g = built.Generated(int(f["kind"]), seed=1, param=int(f["param"]))
+    o = Oracle(g.desc)
+    cam = camera_from(f["camera"])
+    w, h, spp, seed = int(f["width"]), int(f["height"]), int(f["spp"]), int(f["seed"])
+    img, aux, rays = o.render(cam, w, h, spp, 10, seed=seed, rng_mode=2, aux=True)
+    assert img.tobytes() == f["image"].tobytes()
+    assert aux.tobytes() == f["aux"].tobytes()
+    assert rays == int(f["rays"])
+    img2, aux2, rays2 = o.render(cam, w, h, spp, 10, seed=seed, rng_mode=1, states=f["states"], aux=True)
+    assert img2.tobytes() == f["image"].tobytes() and rays2 == rays
+
+
+def test_oracle_matches_reference_live(built):
+    from oracle.oracle import Oracle, Reference, ref_available
+    if not ref_available():
+        pytest.skip("reference harness absent")
+    from photon_tracer_b200 import abi
+    for kind, param, seed in [(abi.PT_GEN_ROOM_MESH, 3, 11), (abi.PT_GEN_REF_MATERIALS, 0, 1),
+                              (abi.PT_GEN_INSTANCES, 150, 4), (abi.PT_GEN_BATCH_SCENE, 0, 23)]:
+        g = built.Generated(kind, seed=seed, param=param)
+        o, r = Oracle(g.desc), Reference(g.desc)
+        rays = built.generate_rays(seed, [-4, -1, -4], [4, 3, 4], 5000)
+        ho = o.trace_closest(rays)
+        hr, bad = r.trace_closest(rays)
+        assert bad == 0 and ho.tobytes() == hr.tobytes()
+        assert np.array_equal(o.trace_any(rays, 0.001, 3.0), r.trace_any(rays, 0.001, 3.0))
+        io, ao, ro = o.render(g.camera, 24, 16, 3, 10, seed=seed, rng_mode=2, aux=True, first_sample=5)
+        ir, ar, rr = r.render(g.camera, 24, 16, 3, 10, seed=seed, aux=True, first_sample=5)
+        assert io.tobytes() == ir.tobytes() and ao.tobytes() == ar.tobytes() and ro == rr
+
+
+def test_oracle_no_bvh_matches_reference(built):
+    """The reference's plain-list mode (geometry::build(false)) is the default for materials."""
+    from oracle.oracle import Oracle, Reference, ref_available
+    if not ref_available():
+        pytest.skip("reference harness absent")
+    from photon_tracer_b200 import abi
+    g = built.Generated(abi.PT_GEN_REF_FIELD, seed=1, use_bvh=0)
+    o, r = Oracle(g.desc), Reference(g.desc)
+    rays = built.generate_rays(3, [-3, -0.5, -3], [3, 2, 1], 4000)
+    assert o.trace_closest(rays).tobytes() == r.trace_closest(rays)[0].tobytes()
+
+
+def test_sampler_known_answers(built):
+    """The Sobol pairs (sampler.hpp) of the oracle against the reference's, and
+    the superset-XOR form of the second Sobol dimension the GPU computes."""
+    from oracle.oracle import oracle_sample_2d, ref_available, ref_sample_2d
+    rng = np.random.default_rng(0)
+    cases = [(int(rng.integers(0, 2**63)), int(rng.integers(0, 4000)), int(rng.integers(0, 3000)),
+              int(rng.integers(0, 2**20)), int(b), int(po)) for b, po in [(-1, 0), (0, 0), (0, 1), (1, 0), (1, 1)]
+             for _ in range(40)]
+    if ref_available():
+        for c in cases:
+            assert np.array_equal(oracle_sample_2d(*c), ref_sample_2d(*c)), c
+
+    def table_sobol(i):
+        v = [1 << 31]
+        for k in range(1, 32):
+            v.append(v[-1] ^ (v[-1] >> 1))
+        r = 0
+        for k in range(32):
+            if i >> k & 1:
+                r ^= v[k]
+        return int(f"{r:032b}"[::-1], 2)
+
+    def superset_xor(r):
+        r ^= (r >> 1) & 0x55555555
+        r ^= (r >> 2) & 0x33333333
+        r ^= (r >> 4) & 0x0F0F0F0F
+        r ^= (r >> 8) & 0x00FF00FF
+        r ^= (r >> 16) & 0x0000FFFF
+        return r
+
+    for i in [0, 1, 2, 3, 0xFFFFFFFF, 0x80000000] + [int(x) for x in rng.integers(0, 2**32, 2000)]:
+        assert table_sobol(i) == superset_xor(i), hex(i)
+
+
+def test_generators_match_reference_scenes(built):
+    """materials / field / room built by the library equal the reference's make_scene / make_room_scene."""
+    import ctypes as C
+    from oracle.oracle import ref_available, ref_lib
+    if not ref_available():
+        pytest.skip("reference harness absent")
+    from photon_tracer_b200 import abi
+    for gen, sid in [(abi.PT_GEN_REF_MATERIALS, 0), (abi.PT_GEN_REF_FIELD, 1), (abi.PT_GEN_REF_ROOM, 3)]:
+        g = built.Generated(gen)
+        a = abi.desc_arrays(g.desc)
+        counts = (C.c_uint32 * 4)()
+        ref_lib().ref_builtin_scene(sid, counts, None, None)
+        sph = np.zeros((counts[0], 4), np.float32)
+        tri = np.zeros((counts[2], 9), np.float32)
+        ref_lib().ref_builtin_scene(sid, counts, sph.ctypes.data_as(C.c_void_p), tri.ctypes.data_as(C.c_void_p))
+        assert counts[0] == len(a["spheres"]) and counts[1] == len(a["large_spheres"]) and counts[2] == len(a["triangles"])
+        mine_s = np.concatenate([a["spheres"]["center"], a["spheres"]["radius"][:, None]], axis=1)
+        assert mine_s.tobytes() == sph.tobytes()
+        mine_t = np.concatenate([a["triangles"]["p0"], a["triangles"]["e1"], a["triangles"]["e2"]], axis=1)
+        assert mine_t.tobytes() == tri.tobytes()
+
+
+def test_generated_fields_match_reference_constructors(built):
+    """e1, e2, face normal (triangle ctor) and to_object (affine::inverse) as the reference computes them."""
+    import ctypes as C
+    from oracle.oracle import Reference, ref_available
+    if not ref_available():
+        pytest.skip("reference harness absent")
+    from photon_tracer_b200 import abi
+    g = built.Generated(abi.PT_GEN_INSTANCES, seed=3, param=200)
+    r = Reference(g.desc)
+    a = abi.desc_arrays(g.desc)
+    out = np.zeros(12, np.float32)
+    for m, tris in enumerate(a["meshes"]):
+        for i in range(0, len(tris), max(1, len(tris) // 200)):
+            r.lib.ref_triangle_fields(r.h, m, i, out.ctypes.data_as(C.c_void_p))
+            mine = np.concatenate([tris[i]["p0"], tris[i]["e1"], tris[i]["e2"], tris[i]["face_normal"]])
+            assert mine.tobytes() == out.tobytes()
+    for k in range(len(a["instances"])):
+        r.lib.ref_instance_to_object(r.h, k, out.ctypes.data_as(C.c_void_p))
+        x = a["instances"][k]["to_object"]
+        assert np.concatenate([x["m"].ravel(), x["t"]]).tobytes() == out.tobytes()
+
+
+def block_z(image, mean, sigma, seeds, block=20, floor=2e-4):
+    """render_test.py's check_scene statistics: worst |z| per block, per block
+    row and per image channel against the fixture (tests/render_test.py:151-182)."""
+    h, w, _ = image.shape
+    bw, bh = w // block, h // block
+    means = image[:bh * block, :bw * block].reshape(bh, block, bw, block, 3).mean(axis=(1, 3), dtype=np.float64)
+    diffs = means.reshape(-1) - mean
+    scale = np.sqrt(1 + 1 / seeds)
+    var = (np.maximum(sigma, floor) * scale) ** 2
+    worst_block = np.max(np.abs(diffs) / np.sqrt(var))
+    d3, v3 = diffs.reshape(bh, bw, 3), var.reshape(bh, bw, 3)
+    worst_row = np.max(np.abs(d3.sum(axis=1)) / np.sqrt(v3.sum(axis=1)))
+    image_z = d3.sum(axis=(0, 1)) / np.sqrt(v3.sum(axis=(0, 1)))
+    return worst_block, worst_row, np.max(np.abs(image_z))
+
+
+def test_reference_fixture_is_reproduced_by_reference_on_generated_scene(built):
+    """The reference, rendering the library's rebuild of its materials scene,
+    passes its own statistical fixture (tests/reference.json thresholds)."""
+    from oracle.oracle import Reference, ref_available
+    if not ref_available():
+        pytest.skip("reference harness absent")
+    import json
+    from photon_tracer_b200 import abi
+    f = golden("reference_blocks.npz")
+    meta = json.loads(str(f["meta"]))
+    g = built.Generated(abi.PT_GEN_REF_MATERIALS)
+    img, _, _ = Reference(g.desc).render(g.camera, meta["width"], meta["width"] * 9 // 16, meta["spp"], 10, seed=1,
+                                        threads=os.cpu_count())
+    b, r, i = block_z(img, f["materials_mean"], f["materials_sigma"], meta["seeds"])
+    assert b <= 10 and r <= 6 and i <= 5, (b, r, i)

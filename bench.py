@@ -135,10 +135,11 @@ def cpu_reference_rate(desc, cam, seconds: float, threads: int):
     else:
         o, kind, threads = Oracle(desc), "port", 1
         run = lambda j0, n: o.render(cam, WIDTH, HEIGHT, SPP, DEPTH, seed=SEED, rng_mode=2, row0=j0, rows=n)[2]
+    calib = max(1, threads // 2)
     t0 = time.perf_counter()
-    rays = run(HEIGHT // 2, max(1, threads // 4))
+    run(HEIGHT // 2, calib)
     dt = time.perf_counter() - t0
-    rows = int(max(threads, min(HEIGHT, (max(1, threads // 4)) * seconds / max(dt, 1e-3))))
+    rows = int(max(threads, min(HEIGHT, calib * seconds / max(dt, 1e-3))))
     j0 = max(0, HEIGHT // 2 - rows // 2)
     t0 = time.perf_counter()
     rays = run(j0, rows)
@@ -189,6 +190,27 @@ def run_reference_arm(args, rank, world):
     return 0
 
 
+def run_profile_case(args):
+    """A small frame of the same scene (256x256, 16 spp), rendered three times
+    with the chosen kernel: the case ncu captures are taken on."""
+    import torch
+    import photon_tracer_b200 as pt
+    from photon_tracer_b200 import abi
+    g = pt.Generated(abi.PT_GEN_ROOM_MESH, seed=SEED)
+    scene = pt.Scene(g)
+    mode = abi.PT_MODE_MEGAKERNEL if args.mode == "mega" else abi.PT_MODE_WAVEFRONT
+    w = h = 256
+    st = pt.Scene.settings(w, h, 16, DEPTH, SEED, 0, mode, abi.PT_RNG_SAMPLE)
+    out = torch.empty((h, w, 3), dtype=torch.float32, device="cuda")
+    rays = torch.zeros(1, dtype=torch.int64, device="cuda")
+    stream = torch.cuda.current_stream().cuda_stream
+    for _ in range(3):
+        scene.render_device(g.camera, st, out.data_ptr(), 0, rays.data_ptr(), stream)
+    scene.sync(stream)
+    print(json.dumps({"profile_case": f"{w}x{h} at 16 spp x3", "mode": args.mode, "rays": int(rays.item())}))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
     ap.add_argument("--gpus", type=int, default=1)
@@ -197,6 +219,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--mode", default="mega", choices=["mega", "wave"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile-case", action="store_true",
+                    help="the small case profiles are taken on: 256x256 at 16 spp, 3 frames, no baselines")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -207,6 +231,8 @@ def main():
 
     if args.impl == "reference":
         return run_reference_arm(args, rank, world)
+    if args.profile_case:
+        return run_profile_case(args)
 
     import torch
     import torch.distributed as dist

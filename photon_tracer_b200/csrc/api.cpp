@@ -10,6 +10,7 @@
 #include <string>
 
 #include "kernels.h"
+#include "wavefront.h"
 #include "scene_host.hpp"
 
 namespace pt {
@@ -66,7 +67,8 @@ struct pt_scene {
     unsigned int* work = nullptr;      // megakernel work counter
     unsigned long long* rays = nullptr;
     cudaStream_t stream = nullptr;
-    Scratch out, aux, states, in_rays, out_hits, counts;
+    Scratch out, aux, states, in_rays, out_hits, counts, wave;
+    uint32_t* host_counts = nullptr;  // pinned, for the wavefront queue read-back
     int blocks_per_sm[4] = {0, 0, 0, 0};
 };
 
@@ -140,8 +142,20 @@ PtRenderParams make_params(const pt_camera* cam, const pt_settings* st) {
     return p;
 }
 
+// Paths the wavefront keeps in flight: one per pixel up to 2^20.
+constexpr uint32_t kMaxWaveSlots = 1u << 20;
+
 pt_status launch_render(pt_scene* s, PtRenderParams& p, int mode, cudaStream_t stream) {
-    (void)mode;  // the megakernel serves every mode until the wavefront path lands
+    if (mode == PT_MODE_WAVEFRONT) {
+        const uint64_t px = uint64_t(p.width) * uint64_t(p.rows);
+        const uint32_t slots = uint32_t(px < kMaxWaveSlots ? px : kMaxWaveSlots);
+        if (pt_status e = s->wave.ensure(pt_wavefront_bytes(slots), "wavefront state")) return e;
+        if (!s->host_counts)
+            if (cudaError_t e = cudaMallocHost(&s->host_counts, 256)) return cuda_fail(e, "wavefront counters");
+        if (cudaError_t e = pt_launch_wavefront(s->dev, p, s->wave.ptr, slots, s->sms, stream, s->host_counts))
+            return cuda_fail(e, "wavefront");
+        return PT_OK;
+    }
     if (cudaError_t e = cudaMemsetAsync(s->work, 0, sizeof(unsigned int), stream)) return cuda_fail(e, "render");
     const int variant = (p.aux ? 1 : 0) + (p.rng_mode == PT_RNG_SNAPSHOT ? 2 : 0);
     PtLaunchShape shape;
@@ -283,6 +297,8 @@ pt_status pt_scene_destroy(pt_scene* s) {
     s->in_rays.release();
     s->out_hits.release();
     s->counts.release();
+    s->wave.release();
+    if (s->host_counts) cudaFreeHost(s->host_counts);
     if (s->stream) cudaStreamDestroy(s->stream);
     if (s->arena) cudaFree(s->arena);
     delete s;

@@ -19,7 +19,7 @@ namespace ptd {
 struct V {
     float x, y, z;
 };
-__device__ __forceinline__ V mk(float x, float y, float z) { return {x, y, z}; }
+__host__ __device__ __forceinline__ V mk(float x, float y, float z) { return {x, y, z}; }
 __device__ __forceinline__ V operator+(V a, V b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
 __device__ __forceinline__ V operator-(V a, V b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
 __device__ __forceinline__ V operator-(V a) { return {-a.x, -a.y, -a.z}; }

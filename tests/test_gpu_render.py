@@ -180,3 +180,34 @@ def test_denoise_matches_oracle(pt):
     got = pt.denoise_atrous(img, albedo, normal, variance)
     want = oracle_denoise(img, albedo, normal, variance)
     np.testing.assert_allclose(got, want, rtol=1e-3, atol=1e-5)
+
+
+@pytest.mark.parametrize("kind,param,w,h,spp,aux", [
+    ("ROOM_MESH", 6, 96, 64, 4, True), ("RANDOM_SPHERES", 0, 80, 45, 3, False), ("INSTANCES", 0, 64, 36, 2, True),
+    ("REF_MATERIALS", 0, 50, 30, 5, True),
+])
+def test_wavefront_equals_megakernel(pt, kind, param, w, h, spp, aux):
+    """The wavefront stages run the same per-slot arithmetic in the same order
+    as the megakernel lanes: identical bytes, identical ray count."""
+    from photon_tracer_b200 import abi
+    g = pt.Generated(getattr(abi, "PT_GEN_" + kind), seed=3, param=param)
+    s = pt.Scene(g)
+    a, ax, ra = s.render(g.camera, w, h, spp, 10, seed=5, aux=aux, mode=abi.PT_MODE_MEGAKERNEL)
+    b, bx, rb = s.render(g.camera, w, h, spp, 10, seed=5, aux=aux, mode=abi.PT_MODE_WAVEFRONT)
+    assert a.tobytes() == b.tobytes() and ra == rb
+    if aux:
+        assert ax.tobytes() == bx.tobytes()
+
+
+def test_wavefront_snapshot_and_depth_zero(pt):
+    from photon_tracer_b200 import abi
+    f = golden("ref_render_room_mesh.npz")
+    g = pt.Generated(int(f["kind"]), seed=1, param=int(f["param"]))
+    s = pt.Scene(g)
+    w, h, spp = int(f["width"]), int(f["height"]), int(f["spp"])
+    kw = dict(seed=int(f["seed"]), rng=abi.PT_RNG_SNAPSHOT, states=f["states"], aux=True)
+    a = s.render(camera_from(f["camera"]), w, h, spp, 10, mode=abi.PT_MODE_MEGAKERNEL, **kw)
+    b = s.render(camera_from(f["camera"]), w, h, spp, 10, mode=abi.PT_MODE_WAVEFRONT, **kw)
+    assert a[0].tobytes() == b[0].tobytes() and a[1].tobytes() == b[1].tobytes() and a[2] == b[2]
+    img, ax, rays = s.render(g.camera, 40, 30, 2, 0, seed=1, aux=True, mode=abi.PT_MODE_WAVEFRONT)
+    assert not img.any() and not ax.any() and rays == 0

@@ -191,23 +191,24 @@ def run_reference_arm(args, rank, world):
 
 
 def run_profile_case(args):
-    """A small frame of the same scene (256x256, 16 spp), rendered three times
-    with the chosen kernel: the case ncu captures are taken on."""
+    """The case ncu captures are taken on: the same scene and resolution at
+    4 spp (1/16 of a step's work, so every lane still renders many pixels),
+    rendered three times with the chosen kernel."""
     import torch
     import photon_tracer_b200 as pt
     from photon_tracer_b200 import abi
     g = pt.Generated(abi.PT_GEN_ROOM_MESH, seed=SEED)
     scene = pt.Scene(g)
     mode = abi.PT_MODE_MEGAKERNEL if args.mode == "mega" else abi.PT_MODE_WAVEFRONT
-    w = h = 256
-    st = pt.Scene.settings(w, h, 16, DEPTH, SEED, 0, mode, abi.PT_RNG_SAMPLE)
+    w, h, spp = WIDTH, HEIGHT, 4
+    st = pt.Scene.settings(w, h, spp, DEPTH, SEED, 0, mode, abi.PT_RNG_SAMPLE)
     out = torch.empty((h, w, 3), dtype=torch.float32, device="cuda")
     rays = torch.zeros(1, dtype=torch.int64, device="cuda")
     stream = torch.cuda.current_stream().cuda_stream
     for _ in range(3):
         scene.render_device(g.camera, st, out.data_ptr(), 0, rays.data_ptr(), stream)
     scene.sync(stream)
-    print(json.dumps({"profile_case": f"{w}x{h} at 16 spp x3", "mode": args.mode, "rays": int(rays.item())}))
+    print(json.dumps({"profile_case": f"{w}x{h} at {spp} spp x3", "mode": args.mode, "rays": int(rays.item())}))
     return 0
 
 
@@ -220,7 +221,7 @@ def main():
     ap.add_argument("--mode", default="mega", choices=["mega", "wave"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile-case", action="store_true",
-                    help="the small case profiles are taken on: 256x256 at 16 spp, 3 frames, no baselines")
+                    help="the case profiles are taken on: 1024x1024 at 4 spp, 3 frames, no baselines")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -61,12 +61,31 @@ def build_ref(force=False):
     return REF_LIB
 
 
+def build_shim_check(force=False):
+    """oracle/_ref/shim_check: include/photon_cuda_geometry.hpp driven by the
+    reference's own scenes, linked against the product library."""
+    inc = os.path.join(REFERENCE, "include")
+    out = os.path.join(REF_DIR, "shim_check")
+    lib_dir = os.path.join(ROOT, "photon_tracer_b200")
+    if not os.path.isdir(inc) or not os.path.exists(os.path.join(lib_dir, "libphoton_cuda.so")):
+        return out if os.path.exists(out) else None
+    src = os.path.join(HERE, "shim_check.cpp")
+    deps = [src, os.path.join(ROOT, "include", "photon_cuda.h"), os.path.join(ROOT, "include", "photon_cuda_geometry.hpp"),
+            os.path.join(lib_dir, "libphoton_cuda.so"), __file__]
+    os.makedirs(REF_DIR, exist_ok=True)
+    if force or _stale(out, deps):
+        _run(["g++", "-std=c++17", "-O2", "-pthread", "-ffp-contract=off", "-w", "-I" + inc, "-o", out, src,
+              "-L" + lib_dir, "-lphoton_cuda", "-Wl,-rpath,$ORIGIN/../../photon_tracer_b200"])
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
     ap.add_argument("--force", action="store_true")
     args = ap.parse_args()
     print(build_oracle(args.force))
     print(build_ref(args.force) or "reference checkout absent: oracle/_ref not built")
+    print(build_shim_check(args.force) or "shim check not built")
 
 
 if __name__ == "__main__":

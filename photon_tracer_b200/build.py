@@ -71,25 +71,30 @@ def _run(cmd, verbose):
     return res
 
 
-def build(force: bool = False, verbose: bool = False, ptxas_verbose: bool = False) -> str:
-    """Compiles what changed and links the library; returns its path."""
+def build(force: bool = False, verbose: bool = False, ptxas_verbose: bool = False, defines=(), out_dir=None) -> str:
+    """Compiles what changed and links the library; returns its path.
+    defines (e.g. ["PT_MEGA_MIN_BLOCKS=5"]) and out_dir build a tuning
+    variant elsewhere instead of the in-tree library."""
     if not os.path.exists(NVCC):
         raise RuntimeError(f"nvcc not found at {NVCC}")
-    os.makedirs(BUILD, exist_ok=True)
+    build_dir = os.path.join(out_dir, "_build") if out_dir else BUILD
+    lib_path = os.path.join(out_dir, "libphoton_cuda.so") if out_dir else LIB
+    dflags = ["-D" + d for d in defines]
+    os.makedirs(build_dir, exist_ok=True)
     cu, cpp = _sources()
     headers = _headers()
     jobs, objs = [], []
     for src in cu:
-        obj = os.path.join(BUILD, os.path.basename(src) + ".o")
+        obj = os.path.join(build_dir, os.path.basename(src) + ".o")
         objs.append(obj)
         if force or _stale(obj, [src] + headers):
             extra = ["-Xptxas", "-v"] if ptxas_verbose else []
-            jobs.append([NVCC] + NVCC_FLAGS + extra + ["-c", src, "-o", obj])
+            jobs.append([NVCC] + NVCC_FLAGS + dflags + extra + ["-c", src, "-o", obj])
     for src in cpp:
-        obj = os.path.join(BUILD, os.path.basename(src) + ".o")
+        obj = os.path.join(build_dir, os.path.basename(src) + ".o")
         objs.append(obj)
         if force or _stale(obj, [src] + headers):
-            jobs.append(["g++"] + CXX_FLAGS + ["-c", src, "-o", obj])
+            jobs.append(["g++"] + CXX_FLAGS + dflags + ["-c", src, "-o", obj])
     outputs = []
     if jobs:
         with cf.ThreadPoolExecutor(max_workers=min(8, len(jobs))) as ex:
@@ -97,12 +102,12 @@ def build(force: bool = False, verbose: bool = False, ptxas_verbose: bool = Fals
     if ptxas_verbose:
         for r in outputs:
             sys.stdout.write(r.stderr)
-    if force or jobs or _stale(LIB, objs):
-        tmp = LIB + ".tmp"
+    if force or jobs or _stale(lib_path, objs):
+        tmp = lib_path + ".tmp"
         _run([NVCC] + ARCH + ["-shared", "-o", tmp] + objs + ["-lcudart_static", "-lrt", "-ldl", "-lpthread"],
              verbose)
-        shutil.move(tmp, LIB)
-    return LIB
+        shutil.move(tmp, lib_path)
+    return lib_path
 
 
 def main():

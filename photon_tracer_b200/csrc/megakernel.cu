@@ -19,8 +19,14 @@ namespace {
 
 constexpr int kTileW = 8, kTileH = 4;
 
+// Resident 128-thread blocks per SM the register allocation targets (3:
+// at most 168 registers; measured best of 1..6 on the 1024x1024 room frame).
+#ifndef PT_MEGA_MIN_BLOCKS
+#define PT_MEGA_MIN_BLOCKS 3
+#endif
+
 template <bool AUX, bool SNAP>
-__global__ void __launch_bounds__(128) megakernel(PtSceneDev S, PtRenderParams P, uint32_t tiles_x,
+__global__ void __launch_bounds__(128, PT_MEGA_MIN_BLOCKS) megakernel(PtSceneDev S, PtRenderParams P, uint32_t tiles_x,
                                                   uint32_t total_items) {
     StackEntry stack[PT_STACK_MAX];
     const int lane = threadIdx.x & 31;

@@ -6,7 +6,8 @@
 //              reference's bvh::node layout (include/bvh.hpp:27-32: lo[axis][child],
 //              hi[axis][child], first[4], count[4]) with first[] rebased into the
 //              arena. A leaf count word carries PT_LEAF_HAS_SPHERE in bit 31
-//              when the leaf holds at least one sphere.
+//              when the leaf holds at least one sphere, and PT_LEAF_INSTANCES in
+//              bit 30 for leaves of the instance tree.
 //   slots      leaf entries in leaf order, 48 B each, so that a leaf's primitives
 //              are contiguous and need no order[] indirection:
 //                triangle: (p0.xyz, e1.x) (e1.yz, e2.xy) (e2.z, ref, 0, 0)
@@ -21,7 +22,8 @@
 #include <stdint.h>
 
 #define PT_LEAF_HAS_SPHERE 0x80000000u
-#define PT_COUNT_MASK 0x7fffffffu
+#define PT_LEAF_INSTANCES 0x40000000u   // a leaf of the instance tree (entries are instance slots)
+#define PT_COUNT_MASK 0x3fffffffu
 #define PT_SLOT_SPHERE 0x80000000u
 #define PT_NONE 0xffffffffu
 

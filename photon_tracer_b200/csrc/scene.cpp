@@ -48,7 +48,8 @@ pt_status check_tree(const pt_bvh& t, uint32_t n_prims, const char* what) {
 // Appends a tree's nodes, rebased: interior children by node_base, leaves by
 // slot_base; leaf count words get PT_LEAF_HAS_SPHERE from has_sphere(slot).
 template <class HasSphere>
-uint32_t append_nodes(HostArena& A, const std::vector<pt_bvh_node>& nodes, uint32_t slot_base, HasSphere&& has_sphere) {
+uint32_t append_nodes(HostArena& A, const std::vector<pt_bvh_node>& nodes, uint32_t slot_base, HasSphere&& has_sphere,
+                      uint32_t leaf_flags = 0) {
     if (nodes.empty()) return PT_NONE;
     const uint32_t node_base = uint32_t(A.nodes.size() / 32);
     const float inf = std::numeric_limits<float>::infinity();
@@ -66,7 +67,7 @@ uint32_t append_nodes(HostArena& A, const std::vector<pt_bvh_node>& nodes, uint3
                 bool sph = false;
                 for (uint32_t k = 0; k < count; ++k) sph |= has_sphere(first + k);
                 first += slot_base;
-                count |= sph ? PT_LEAF_HAS_SPHERE : 0u;
+                count |= (sph ? PT_LEAF_HAS_SPHERE : 0u) | leaf_flags;
             } else if (n.lo[0][c] != inf) {
                 first += node_base;
             }
@@ -294,7 +295,7 @@ pt_status build_arena(const pt_scene_desc& d, HostArena& A) {
                 affine_box(d.instances[k].to_world, mesh_bounds[d.instances[k].mesh].data(), &boxes[6 * size_t(k)]);
             build_bvh(boxes.data(), d.n_instances, nodes, order);
         }
-        A.inst_root = append_nodes(A, nodes, 0, [](uint32_t) { return false; });
+        A.inst_root = append_nodes(A, nodes, 0, [](uint32_t) { return false; }, PT_LEAF_INSTANCES);
         for (uint32_t k : order) push_islot(k);
         depth_inst = tree_depth(nodes, 0);
     } else {

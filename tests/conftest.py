@@ -29,5 +29,6 @@ def built():
     pbuild.build()
     obuild.build_oracle()
     obuild.build_ref()
+    obuild.build_shim_check()
     import photon_tracer_b200
     return photon_tracer_b200

@@ -122,3 +122,19 @@ def test_rays_generator_is_deterministic(built):
     assert np.all(np.abs(a[:, :3]) <= 1)
     n = np.linalg.norm(a[:, 3:].astype(np.float64), axis=1)
     assert np.allclose(n, 1, atol=1e-6)
+
+
+def test_geometry_bridge_compiles_and_reports_no_device(built):
+    """include/photon_cuda_geometry.hpp compiled against the reference's own
+    headers (oracle/_ref/shim_check): without a GPU the upload answers
+    PT_ERR_NO_DEVICE instead of falling back to anything."""
+    import json
+    import torch
+    shim = os.path.join(ROOT, "oracle", "_ref", "shim_check")
+    if not os.path.exists(shim):
+        pytest.skip("reference checkout absent: the bridge check is not built")
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present (the GPU test runs the bridge)")
+    res = subprocess.run([shim, "3"], capture_output=True, text=True, timeout=120)
+    assert res.returncode == 3
+    assert json.loads(res.stdout)["upload"] == 7

@@ -198,3 +198,22 @@ def test_device_buffers_entry_point(pt):
     s.sync(stream)
     got = d_hits.cpu().numpy().view(abi.HIT_DTYPE).reshape(-1)
     assert_hits_equal(got, s.trace_closest(rays), rays)
+
+
+@pytest.mark.parametrize("scene_id", [0, 1, 3])
+def test_geometry_bridge_on_reference_scenes(pt, scene_id):
+    """The reference's own scenes, built by its build_world and handed over
+    through include/photon_cuda_geometry.hpp with the reference's own trees:
+    GPU closest-hit t equals geometry::hit's rec.t on every ray, and the
+    rendered frame's mean agrees with render_row_linear's."""
+    import json
+    import subprocess
+    from conftest import ROOT
+    shim = os.path.join(ROOT, "oracle", "_ref", "shim_check")
+    if not os.path.exists(shim):
+        pytest.skip("the bridge check binary was not built (needs the reference checkout at build time)")
+    res = subprocess.run([shim, str(scene_id)], capture_output=True, text=True, timeout=600)
+    out = json.loads(res.stdout)
+    assert res.returncode == 0 and out["hit_mismatch"] == 0, out
+    assert abs(out["gpu_mean"] - out["cpu_mean"]) <= 0.02 * out["cpu_mean"], out
+    assert abs(out["gpu_rays"] - out["cpu_rays"]) <= 0.02 * out["cpu_rays"], out

@@ -290,6 +290,22 @@ pt_status pt_denoise_atrous_device(int width, int height, const float* d_color, 
 /* Scratch floats pt_denoise_atrous_device needs for a width x height frame. */
 size_t pt_denoise_atrous_scratch_floats(int width, int height);
 
+/* No counterpart in the reference. The filter of pt_denoise_atrous_device for
+ * callers that cannot allocate device memory (a host that owns all device
+ * memory through its own pool, a frame loop where cudaMalloc -- which can
+ * synchronise and can fail -- is not allowed): it calls no allocator and
+ * takes its scratch from a fixed array inside the library, which every GPU
+ * that loads the library holds (11.5 MB) until the process exits. Frames of
+ * more than PT_ATROUS_NOALLOC_MAX_PIXELS pixels are refused with
+ * PT_ERR_INVALID_ARG. The first call on each device looks up the array's
+ * device address (make it before any stream capture). All calls share the
+ * array: calls whose work overlaps on the GPU (other streams, other threads)
+ * race and corrupt each other's output. Device buffers, enqueued on stream. */
+#define PT_ATROUS_NOALLOC_MAX_PIXELS 262144
+pt_status pt_denoise_atrous_device_noalloc(int width, int height, const float* d_color, const float* d_albedo,
+                                           const float* d_normal, const float* d_variance, float* d_out,
+                                           void* stream);
+
 /* ---- procedural scenes and ray sets (no reference counterpart) ---------------- */
 /* Generators for the benchmark workloads and the reference's own scenes
  * (materials, field, room: include/renderer.hpp:158-208, 245-268). */

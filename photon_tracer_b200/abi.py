@@ -150,6 +150,7 @@ PROTOTYPES = [
     ("pt_denoise_atrous", ST, [C.c_int, C.c_int, P, P, P, P, P]),
     ("pt_denoise_atrous_device", ST, [C.c_int, C.c_int, P, P, P, P, P, P, P]),
     ("pt_denoise_atrous_scratch_floats", SIZE, [C.c_int, C.c_int]),
+    ("pt_denoise_atrous_device_noalloc", ST, [C.c_int, C.c_int, P, P, P, P, P, P]),
     ("pt_generate", ST, [C.POINTER(pt_gen_params), C.POINTER(P)]),
     ("pt_generated_desc", C.POINTER(pt_scene_desc), [P]),
     ("pt_generated_camera", C.POINTER(pt_camera), [P]),

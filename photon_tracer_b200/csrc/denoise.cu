@@ -156,3 +156,61 @@ pt_status pt_denoise_atrous(int w, int h, const float* color, const float* albed
 }
 
 }  // extern "C"
+
+// ---- the filter without any allocation ------------------------------------------------------
+// Some callers of this library cannot call cudaMalloc: a host application that
+// owns all device memory through its own pool and does not let plugins
+// allocate, or a per-frame loop where an allocation -- which can synchronise
+// the device and can fail under memory pressure -- is not allowed. For them
+// pt_denoise_atrous_device_noalloc runs the same filter with its scratch in
+// the array below, a fixed part of the library's device image: every GPU that
+// loads the library holds these 11.5 MB until the process exits, and frames
+// are limited to PT_ATROUS_NOALLOC_MAX_PIXELS pixels.
+//
+// Host code must not hand g_atrous_scratch to a kernel: here its name is only
+// a host-side stand-in. The device address is looked up once per device, with
+// that device current, by the first call on it (cudaGetSymbolAddress), so the
+// first call on each device should come before any stream capture. Every call
+// uses the same array and leaves the last call's data in it; the filter writes
+// every scratch value before reading it, so nothing needs clearing, but two
+// calls whose work overlaps on the GPU (different streams, or different host
+// threads on one device) race on the array and corrupt each other's output.
+static __device__ __align__(256) float g_atrous_scratch[11 * size_t(PT_ATROUS_NOALLOC_MAX_PIXELS)];
+
+#include <map>
+#include <mutex>
+
+namespace {
+std::mutex g_scratch_lock;
+std::map<int, float*> g_scratch_addr;  // device ordinal -> device address of g_atrous_scratch
+}  // namespace
+
+extern "C" pt_status pt_denoise_atrous_device_noalloc(int w, int h, const float* color, const float* albedo,
+                                                      const float* normal, const float* variance, float* out,
+                                                      void* stream) {
+    pt::clear_error();
+    if (w <= 0 || h <= 0) return pt::fail(PT_ERR_INVALID_ARG, "pt_denoise_atrous_device_noalloc: bad size");
+    if (size_t(w) * size_t(h) > size_t(PT_ATROUS_NOALLOC_MAX_PIXELS))
+        return pt::fail(PT_ERR_INVALID_ARG,
+                        "pt_denoise_atrous_device_noalloc: " + std::to_string(w) + "x" + std::to_string(h) +
+                            " is more than the " + std::to_string(PT_ATROUS_NOALLOC_MAX_PIXELS) +
+                            " pixels its built-in scratch holds; use pt_denoise_atrous_device with your own scratch");
+    if (!color || !albedo || !normal || !variance || !out)
+        return pt::fail(PT_ERR_INVALID_ARG, "pt_denoise_atrous_device_noalloc: null pointer");
+    int dev = 0;
+    if (pt_status st = cuda_status(cudaGetDevice(&dev), "pt_denoise_atrous_device_noalloc")) return st;
+    float* scratch = nullptr;
+    {
+        std::lock_guard<std::mutex> lock(g_scratch_lock);
+        auto it = g_scratch_addr.find(dev);
+        if (it == g_scratch_addr.end()) {
+            void* p = nullptr;
+            if (pt_status st = cuda_status(cudaGetSymbolAddress(&p, g_atrous_scratch),
+                                           "pt_denoise_atrous_device_noalloc: scratch address"))
+                return st;
+            it = g_scratch_addr.emplace(dev, static_cast<float*>(p)).first;
+        }
+        scratch = it->second;
+    }
+    return pt_denoise_atrous_device(w, h, color, albedo, normal, variance, out, scratch, stream);
+}

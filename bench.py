@@ -212,6 +212,115 @@ def run_profile_case(args):
     return 0
 
 
+def run_batch_workload(args):
+    """64 scenes (batch generator seeds 1..64) in one
+    persistent launch from a CUDA graph, the strategy picked by the
+    autotuner, against one megakernel launch per scene."""
+    import torch
+    import photon_tracer_b200 as pt
+    from photon_tracer_b200 import abi
+    t0 = time.perf_counter()
+    items = pt.batch_scenes(64)
+    build_s = time.perf_counter() - t0
+    auto = pt.Batch(items, abi.PT_BATCH_AUTO)
+    auto.render()  # tunes
+    info = auto.info()
+    seq = pt.Batch(items, abi.PT_BATCH_PER_SCENE_MEGA)
+    one = pt.Batch(items, abi.PT_BATCH_ONE_LAUNCH)
+
+    def timed(b, k):
+        ms = []
+        for _ in range(args.warmup):
+            b.render(count_rays=False)
+        torch.cuda.synchronize()
+        rays = 0
+        for _ in range(k):
+            t = time.perf_counter()
+            rays = b.render()
+            ms.append((time.perf_counter() - t) * 1e3)
+        return statistics.median(ms), rays, b.scene_times()
+    ms_one, rays_one, times_one = timed(one, args.steps)
+    ms_seq, rays_seq, times_seq = timed(seq, args.steps)
+    samples = int(info.total_samples)
+    line = {"workload": "batch", "metric": "samples/s (64-scene batch)", "unit": "Msamples/s",
+            "value": round(samples / (ms_one / 1e3) / 1e6, 1), "steps": args.steps, "warmup": args.warmup,
+            "config": {"scenes": 64, "generator": "batch scenes, seeds 1..64", "total_pixels": int(info.total_pixels),
+                       "total_samples": samples, "host_build_s": round(build_s, 2)},
+            "one_launch": {"ms": round(ms_one, 2), "Mrays_s": round(rays_one / ms_one / 1e3, 1),
+                           "scene_done_ms_median": round(float(np.median(times_one)), 2),
+                           "scene_done_ms_max": round(float(np.max(times_one)), 2)},
+            "per_scene_launches": {"ms": round(ms_seq, 2), "Mrays_s": round(rays_seq / ms_seq / 1e3, 1),
+                                   "scene_done_ms_median": round(float(np.median(times_seq)), 2),
+                                   "scene_done_ms_max": round(float(np.max(times_seq)), 2)},
+            "autotuner": {"choice": {1: "one launch", 2: "per-scene megakernel", 3: "per-scene wavefront"}[info.strategy],
+                          "threads": info.threads, "tune_ms": [round(x, 2) for x in info.tune_ms],
+                          "candidates": ["one launch x64", "one launch x128", "one launch x256",
+                                         "per-scene megakernel", "per-scene wavefront"]},
+            "speedup_one_launch_vs_per_scene": round(ms_seq / ms_one, 3), "timing": "wall clock around the blocking render"}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_convergence_workload(args):
+    """The headline study at 1920x1080: time to reach relMSE <= 0.01 against
+    FP64 ground truth for plain path tracing and for path tracing followed by
+    the a-trous filter, on held-out seeds of the random-spheres generator."""
+    import photon_tracer_b200 as pt
+    from photon_tracer_b200 import abi, metrics
+    w, h = 1920, 1080
+    results = []
+    for seed in args.seeds:
+        g = pt.Generated(abi.PT_GEN_RANDOM_SPHERES, seed=seed)
+        cam = pt.camera_look_at((13, 2, 3), (0, 0, 0), 20.0, w / h)
+        scene = pt.Scene(g)
+        gt = metrics.GroundTruth(scene, cam, w, h, seed=seed, pass_spp=256)
+        t = time.perf_counter()
+        gt.add(max(1, args.gt_spp // 256))
+        gt_s = time.perf_counter() - t
+        truth = gt.image()
+        plain = metrics.time_to_error(scene, cam, w, h, truth, seed=seed, denoise=None)
+        den = metrics.time_to_error(scene, cam, w, h, truth, seed=seed, denoise="atrous", max_spp=1024)
+        results.append({"seed": seed, "gt_spp": gt.spp, "gt_s": round(gt_s, 2), "plain": plain, "atrous": den})
+    line = {"workload": "convergence", "metric": "1080p time-to-relMSE<=0.01, denoised vs plain GPU PT", "unit": "ms",
+            "higher_is_better": False, "results": results,
+            "note": "ground truth = FP64 per-pixel sums of gt_spp samples (numbered apart from the tested ones); "
+                    "times are GPU event times of render (+ filter)"}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_scene_workload(args, kind, label, param=0):
+    """Mrays/s of the megakernel on another BASELINE configuration."""
+    import torch
+    import photon_tracer_b200 as pt
+    from photon_tracer_b200 import abi
+    g = pt.Generated(kind, seed=SEED, param=param)
+    scene = pt.Scene(g)
+    st = pt.Scene.settings(g.width, g.height, g.spp, DEPTH, SEED, 0, abi.PT_MODE_MEGAKERNEL, abi.PT_RNG_SAMPLE)
+    out = torch.empty((g.height, g.width, 3), dtype=torch.float32, device="cuda")
+    rays = torch.zeros(1, dtype=torch.int64, device="cuda")
+    stream = torch.cuda.current_stream().cuda_stream
+    for _ in range(args.warmup):
+        scene.render_device(g.camera, st, out.data_ptr(), 0, rays.data_ptr(), stream)
+    scene.sync(stream)
+    rays.zero_()
+    ms = []
+    for _ in range(args.steps):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        scene.render_device(g.camera, st, out.data_ptr(), 0, rays.data_ptr(), stream)
+        b.record()
+        torch.cuda.synchronize()
+        ms.append(a.elapsed_time(b))
+    scene.sync(stream)
+    total = sum(ms)
+    print(json.dumps({"workload": label, "metric": METRIC, "unit": "Mrays/s",
+                      "value": round(int(rays.item()) / total / 1e3, 1), "ms_per_step": round(total / len(ms), 2),
+                      "config": {"width": g.width, "height": g.height, "spp": g.spp, "triangles": int(g.desc.n_triangles),
+                                 "instances": int(g.desc.n_instances), "spheres": int(g.desc.n_spheres)}}), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
     ap.add_argument("--gpus", type=int, default=1)
@@ -220,6 +329,10 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--mode", default="mega", choices=["mega", "wave"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default="room", choices=["room", "batch", "convergence", "instances", "spheres"],
+                    help="room: the headline line (config 1); the others print their own JSON line")
+    ap.add_argument("--seeds", type=int, nargs="+", default=[1001, 1002])
+    ap.add_argument("--gt-spp", type=int, default=4096)
     ap.add_argument("--profile-case", action="store_true",
                     help="the case profiles are taken on: 1024x1024 at 4 spp, 3 frames, no baselines")
     args = ap.parse_args()
@@ -234,6 +347,17 @@ def main():
         return run_reference_arm(args, rank, world)
     if args.profile_case:
         return run_profile_case(args)
+    if args.workload != "room":
+        import torch
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        from photon_tracer_b200 import abi as _abi
+        if args.workload == "batch":
+            return run_batch_workload(args)
+        if args.workload == "convergence":
+            return run_convergence_workload(args)
+        if args.workload == "instances":
+            return run_scene_workload(args, _abi.PT_GEN_INSTANCES, "instances")
+        return run_scene_workload(args, _abi.PT_GEN_RANDOM_SPHERES, "spheres")
 
     import torch
     import torch.distributed as dist

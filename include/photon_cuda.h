@@ -306,6 +306,56 @@ pt_status pt_denoise_atrous_device_noalloc(int width, int height, const float* d
                                            const float* d_normal, const float* d_variance, float* d_out,
                                            void* stream);
 
+/* ---- ground truth and images ------------------------------------------------------- */
+/* Adds weight * d_frame[i] to d_sum[i] in FP64 (device buffers, enqueued on
+ * stream): a progressive pass's per-pixel averages times its spp, for
+ * ground-truth sums over many passes (no reference counterpart). */
+pt_status pt_accumulate_pass(const float* d_frame, size_t n_floats, double weight, double* d_sum, void* stream);
+/* write_image (include/image_write.hpp:15-33): PFM for a path ending in .pfm
+ * (linear, bottom row first), else binary PPM of to_display bytes. linear is
+ * 3 floats per pixel, top row first. */
+pt_status pt_write_image(const char* path, int width, int height, const float* linear);
+/* to_display (include/renderer.hpp:421-423): gamma 2, clamped, to a byte. */
+uint8_t pt_to_display(float linear);
+
+/* ---- batched rendering (no reference counterpart) ------------------------------ */
+/* Many scenes of different size, resolution and spp rendered together: their
+ * trees share one device arena and, with PT_BATCH_ONE_LAUNCH, one persistent
+ * launch (captured in a CUDA graph) covers every scene's pixels. Each scene's
+ * image is what pt_render would give for it (PT_RNG_SAMPLE streams). */
+enum { PT_BATCH_AUTO = 0, PT_BATCH_ONE_LAUNCH = 1, PT_BATCH_PER_SCENE_MEGA = 2, PT_BATCH_PER_SCENE_WAVE = 3 };
+typedef struct pt_batch_item {
+    const pt_scene_desc* desc; /* with use_bvh set */
+    pt_camera camera;
+    int32_t width, height, spp, max_bounces;
+    uint64_t seed;
+} pt_batch_item;
+typedef struct pt_batch_info {
+    uint32_t n_scenes;
+    int32_t strategy;   /* the one used (the autotuner's choice for PT_BATCH_AUTO) */
+    int32_t threads;    /* block size of the single launch */
+    int32_t tuned;
+    uint64_t total_pixels, total_samples, device_bytes;
+    double tune_ms[5];  /* autotuner timings: one launch at 64/128/256 threads, per-scene megakernel, per-scene wavefront */
+} pt_batch_info;
+typedef struct pt_batch pt_batch;
+/* Deep-copies the scenes into one arena. PT_BATCH_AUTO measures every
+ * strategy on the first pt_batch_render and keeps the fastest (remembered
+ * for batches of the same shape). */
+pt_status pt_batch_create(const pt_batch_item* items, uint32_t n, int32_t strategy, pt_batch** out);
+/* Renders every scene into the batch's device output, enqueued on stream
+ * (NULL: the batch's own); rays_out (may be NULL) waits and returns the
+ * ray count. */
+pt_status pt_batch_render(pt_batch* batch, void* stream, uint64_t* rays_out);
+/* Scene i's image in device memory (3 floats per pixel, top row first). */
+pt_status pt_batch_output(const pt_batch* batch, uint32_t i, const float** d_image);
+/* Copies scene i's image to host memory (waits for the batch). */
+pt_status pt_batch_download(pt_batch* batch, uint32_t i, float* host);
+/* Completion time of each scene in the last render, ms from its start. */
+pt_status pt_batch_scene_times(pt_batch* batch, double* ms);
+pt_status pt_batch_get_info(const pt_batch* batch, pt_batch_info* info);
+pt_status pt_batch_destroy(pt_batch* batch);
+
 /* ---- procedural scenes and ray sets (no reference counterpart) ---------------- */
 /* Generators for the benchmark workloads and the reference's own scenes
  * (materials, field, room: include/renderer.hpp:158-208, 245-268). */

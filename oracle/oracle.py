@@ -87,6 +87,8 @@ def ref_lib() -> C.CDLL:
         L.ref_camera_roundtrip.restype = C.c_int
         L.ref_camera_roundtrip.argtypes = [C.POINTER(abi.pt_camera)]
         L.ref_builtin_scene.argtypes = [C.c_int, C.POINTER(C.c_uint32), P, P]
+        L.ref_write_image.restype = C.c_int
+        L.ref_write_image.argtypes = [C.c_char_p, C.c_int, C.c_int, P]
         _rlib = L
     return _rlib
 

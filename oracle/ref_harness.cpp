@@ -16,6 +16,7 @@
 #include <thread>
 #include <vector>
 
+#include "image_write.hpp"
 #include "renderer.hpp"
 #include "../include/photon_cuda.h"
 
@@ -336,3 +337,8 @@ void ref_builtin_scene(int id, uint32_t counts[4], float* spheres, float* tris) 
 }
 
 }  // extern "C"
+
+extern "C" {
+// The reference's write_image (include/image_write.hpp:15-33).
+int ref_write_image(const char* path, int w, int h, const float* linear) { return write_image(path, w, h, linear) ? 1 : 0; }
+}

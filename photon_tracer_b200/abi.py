@@ -117,6 +117,19 @@ class pt_gen_params(C.Structure):
                 ("width", C.c_int32), ("height", C.c_int32), ("spp", C.c_int32)]
 
 
+class pt_batch_item(C.Structure):
+    _fields_ = [("desc", C.POINTER(pt_scene_desc)), ("camera", pt_camera), ("width", C.c_int32), ("height", C.c_int32),
+                ("spp", C.c_int32), ("max_bounces", C.c_int32), ("seed", C.c_uint64)]
+
+
+class pt_batch_info(C.Structure):
+    _fields_ = [("n_scenes", C.c_uint32), ("strategy", C.c_int32), ("threads", C.c_int32), ("tuned", C.c_int32),
+                ("total_pixels", C.c_uint64), ("total_samples", C.c_uint64), ("device_bytes", C.c_uint64),
+                ("tune_ms", C.c_double * 5)]
+
+
+PT_BATCH_AUTO, PT_BATCH_ONE_LAUNCH, PT_BATCH_PER_SCENE_MEGA, PT_BATCH_PER_SCENE_WAVE = 0, 1, 2, 3
+
 HIT_DTYPE = np.dtype([("kind", "<u4"), ("index", "<u4"), ("sub", "<u4"), ("t", "<f4"), ("u", "<f4"), ("v", "<f4")])
 NODE_DTYPE = np.dtype([("lo", "<f4", (3, 4)), ("hi", "<f4", (3, 4)), ("first", "<u4", (4,)), ("count", "<u4", (4,))])
 assert HIT_DTYPE.itemsize == C.sizeof(pt_hit)
@@ -151,6 +164,16 @@ PROTOTYPES = [
     ("pt_denoise_atrous_device", ST, [C.c_int, C.c_int, P, P, P, P, P, P, P]),
     ("pt_denoise_atrous_scratch_floats", SIZE, [C.c_int, C.c_int]),
     ("pt_denoise_atrous_device_noalloc", ST, [C.c_int, C.c_int, P, P, P, P, P, P]),
+    ("pt_accumulate_pass", ST, [P, SIZE, C.c_double, P, P]),
+    ("pt_write_image", ST, [C.c_char_p, C.c_int, C.c_int, P]),
+    ("pt_to_display", C.c_uint8, [C.c_float]),
+    ("pt_batch_create", ST, [C.POINTER(pt_batch_item), C.c_uint32, C.c_int32, C.POINTER(P)]),
+    ("pt_batch_render", ST, [P, P, C.POINTER(C.c_uint64)]),
+    ("pt_batch_output", ST, [P, C.c_uint32, C.POINTER(P)]),
+    ("pt_batch_download", ST, [P, C.c_uint32, P]),
+    ("pt_batch_scene_times", ST, [P, C.POINTER(C.c_double)]),
+    ("pt_batch_get_info", ST, [P, C.POINTER(pt_batch_info)]),
+    ("pt_batch_destroy", ST, [P]),
     ("pt_generate", ST, [C.POINTER(pt_gen_params), C.POINTER(P)]),
     ("pt_generated_desc", C.POINTER(pt_scene_desc), [P]),
     ("pt_generated_camera", C.POINTER(pt_camera), [P]),

@@ -205,6 +205,14 @@ def render_row_linear(scene: Scene, cam, j: int, width: int, height: int, sample
                                _ptr(out), seed, first_sample, _ptr(aux)))
 
 
+# ---- images ----------------------------------------------------------------------
+def write_image(path: str, image: np.ndarray) -> None:
+    """write_image (include/image_write.hpp:15-33): PFM for *.pfm, else PPM.
+    image: H x W x 3 linear float32, top row first."""
+    img = np.ascontiguousarray(image, np.float32)
+    check(load().pt_write_image(path.encode(), img.shape[1], img.shape[0], _ptr(img)))
+
+
 # ---- denoising ----------------------------------------------------------------------
 def denoise_atrous(color: np.ndarray, albedo: np.ndarray, normal: np.ndarray, variance: np.ndarray) -> np.ndarray:
     """denoise (include/denoise.hpp:55-139) on the GPU; arrays H x W x {3,3,3,1}."""
@@ -212,4 +220,69 @@ def denoise_atrous(color: np.ndarray, albedo: np.ndarray, normal: np.ndarray, va
     c = [np.ascontiguousarray(a, np.float32) for a in (color, albedo, normal, variance)]
     out = np.empty((h, w, 3), np.float32)
     check(load().pt_denoise_atrous(w, h, *[_ptr(a) for a in c], _ptr(out)))
+    return out
+
+
+# ---- batched rendering ------------------------------------------------------------
+class Batch:
+    """Many scenes rendered together (pt_batch_*): one device arena and, with
+    PT_BATCH_ONE_LAUNCH, one persistent launch replayed from a CUDA graph.
+    items: [(scene_with_desc, camera, width, height, spp, seed), ...] where the
+    scene is a Generated (or anything with .desc_ptr)."""
+
+    def __init__(self, items, strategy: int = abi.PT_BATCH_AUTO, max_bounces: int = 10):
+        lib = load()
+        self._keep = [it[0] for it in items]
+        arr = (abi.pt_batch_item * len(items))()
+        self.sizes = []
+        for i, (scene, cam, w, h, spp, seed) in enumerate(items):
+            arr[i].desc = scene.desc_ptr
+            arr[i].camera = cam
+            arr[i].width, arr[i].height, arr[i].spp, arr[i].max_bounces, arr[i].seed = w, h, spp, max_bounces, seed
+            self.sizes.append((w, h, spp))
+        h = C.c_void_p()
+        check(lib.pt_batch_create(arr, len(items), strategy, C.byref(h)))
+        self._h = h
+
+    def render(self, stream: int = 0, count_rays: bool = True):
+        rays = C.c_uint64()
+        check(load().pt_batch_render(self._h, C.c_void_p(stream or None), C.byref(rays) if count_rays else None))
+        return rays.value
+
+    def image(self, i: int) -> np.ndarray:
+        w, h, _ = self.sizes[i]
+        out = np.empty((h, w, 3), np.float32)
+        check(load().pt_batch_download(self._h, i, _ptr(out)))
+        return out
+
+    def scene_times(self) -> np.ndarray:
+        ms = (C.c_double * len(self.sizes))()
+        check(load().pt_batch_scene_times(self._h, ms))
+        return np.array(list(ms))
+
+    def info(self) -> abi.pt_batch_info:
+        i = abi.pt_batch_info()
+        check(load().pt_batch_get_info(self._h, C.byref(i)))
+        return i
+
+    def close(self):
+        if getattr(self, "_h", None):
+            load().pt_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def batch_scenes(n: int = 64, first_seed: int = 1):
+    """The batched workload: n scenes from seeds first_seed.. of the batch
+    generator (random spheres with 10..2000 spheres or the room with a
+    2..7-subdivision icosphere; 256..1024 square; 4/16/64 spp)."""
+    out = []
+    for s in range(first_seed, first_seed + n):
+        g = Generated(abi.PT_GEN_BATCH_SCENE, seed=s)
+        out.append((g, g.camera, g.width, g.height, g.spp, s))
     return out

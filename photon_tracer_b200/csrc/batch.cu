@@ -1,0 +1,194 @@
+// Batched rendering: many scenes of different size, resolution and spp in one
+// persistent launch over one node arena.
+//
+// The scenes' arenas are merged on the host with every index rebased
+// (batch.cpp), so the arena pointers are shared and a scene differs only by
+// its tree roots, its ranges of large spheres and lights and its flags. Work
+// items are the 8x4 tiles of all scenes' frames in scene order; a lane maps
+// its item to a scene by binary search over the scenes' first items, builds
+// that scene's view of the arena (a few registers) and renders the pixel
+// exactly as the single-scene megakernel does -- same per-pixel stream,
+// same order of sums, so each scene's image is bit-identical to rendering
+// it alone. Each scene's completion time is taken from the global timer
+// when its last pixel is written.
+#include "batch.h"
+#include "path.cuh"
+
+using namespace ptd;
+
+namespace {
+
+constexpr int kTileW = 8, kTileH = 4;
+
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+template <int THREADS>
+__global__ void __launch_bounds__(THREADS, 384 / THREADS) batch_megakernel(PtSceneDev S0, PtBatchLaunch B) {
+    StackEntry stack[PT_STACK_MAX];
+    const int lane = threadIdx.x & 31;
+    if (threadIdx.x == 0) atomicMin(B.start_ns, global_ns());
+
+    unsigned long long rays = 0;
+    bool exhausted = false, has_pixel = false, in_path = false, overflow = false;
+    uint32_t sc = 0;
+    int pi = 0, pj = 0, s = 0, width = 0, height = 0, spp = 0, depth = 0;
+    uint64_t seed = 0;
+    V acc = mk(0, 0, 0);
+    Path path;
+    First first = {mk(0, 0, 0), mk(0, 0, 0)};
+    Sampler smp;
+    Rng rng;
+    PtSceneDev S = S0;
+
+    while (true) {
+        const bool need = !has_pixel && !exhausted;
+        const unsigned want = __ballot_sync(0xffffffffu, need);
+        if (want) {
+            const int leader = __ffs(want) - 1;
+            uint32_t base = 0;
+            if (lane == leader) base = atomicAdd(B.work, uint32_t(__popc(want)));
+            base = __shfl_sync(0xffffffffu, base, leader);
+            if (need) {
+                const uint32_t item = base + __popc(want & ((1u << lane) - 1u));
+                if (item >= B.total_items) {
+                    exhausted = true;
+                } else {
+                    // The scene whose items contain this one.
+                    uint32_t lo = 0, hi = B.n_scenes - 1;
+                    while (lo < hi) {
+                        const uint32_t mid = (lo + hi + 1) >> 1;
+                        if (__ldg(&B.scenes[mid].item_base) <= item) lo = mid;
+                        else hi = mid - 1;
+                    }
+                    sc = lo;
+                    const PtBatchScene& D = B.scenes[sc];
+                    const uint32_t local = item - __ldg(&D.item_base);
+                    const uint32_t tx = __ldg(&D.tiles_x);
+                    width = int(__ldg(&D.width));
+                    height = int(__ldg(&D.height));
+                    const uint32_t tile = local >> 5, l = local & 31u;
+                    pi = int((tile % tx) * kTileW + (l & 7u));
+                    pj = int((tile / tx) * kTileH + (l >> 3));
+                    if (pi < width && pj < height) {
+                        has_pixel = true;
+                        s = 0;
+                        in_path = false;
+                        acc = mk(0, 0, 0);
+                        spp = int(__ldg(&D.spp));
+                        depth = int(__ldg(&D.depth));
+                        seed = __ldg(&D.seed);
+                        S.flat_root = __ldg(&D.flat_root);
+                        S.inst_root = __ldg(&D.inst_root);
+                        S.large = S0.large + __ldg(&D.large_base);
+                        S.large_mat = S0.large_mat + __ldg(&D.large_base);
+                        S.n_large = __ldg(&D.n_large);
+                        S.lights = S0.lights + __ldg(&D.light_base);
+                        S.n_lights = __ldg(&D.n_lights);
+                        S.sky = int(__ldg(&D.sky));
+                        S.sample_lights = int(__ldg(&D.sample_lights));
+                    }
+                }
+            }
+        }
+        if (__all_sync(0xffffffffu, exhausted)) break;
+        if (!has_pixel) continue;
+
+        if (!in_path) {
+            if (depth <= 0) {
+                s = spp;
+            } else {
+                const PtBatchScene& D = B.scenes[sc];
+                const uint32_t idx = uint32_t(s);
+                smp.begin(seed, pi, pj, idx);
+                float du, dv;
+                smp.sample_2d(0, rng, du, dv);
+                const float u = (float(pi) + du) / float(width - 1);
+                const float v = (float(pj) + dv) / float(height - 1);
+                const V origin = mk(__ldg(&D.cam[0]), __ldg(&D.cam[1]), __ldg(&D.cam[2]));
+                const V llc = mk(__ldg(&D.cam[3]), __ldg(&D.cam[4]), __ldg(&D.cam[5]));
+                const V hor = mk(__ldg(&D.cam[6]), __ldg(&D.cam[7]), __ldg(&D.cam[8]));
+                const V ver = mk(__ldg(&D.cam[9]), __ldg(&D.cam[10]), __ldg(&D.cam[11]));
+                path.o = origin;
+                path.d = llc + hor * u + ver * v - origin;
+                path.tp = mk(1, 1, 1);
+                path.rad = mk(0, 0, 0);
+                path.bounce = 0;
+                path.sampled = false;
+                rng.seed(sample_stream_seed(seed, pi, pj, idx));
+                in_path = true;
+            }
+        }
+
+        if (in_path) {
+            ++rays;
+            smp.set_bounce(path.bounce);
+            float t = 1000.0f;
+            Hit h;
+            Counts cnt;
+            Rec rec;
+            if (!closest<false>(S, path.o, path.d, 0.001f, t, h, stack, cnt)) {
+                overflow = true;
+                h.kind = PT_HIT_NONE;
+            }
+            const bool hit = h.kind != PT_HIT_NONE;
+            if (hit) fill(S, h, path.o, path.d, t, rec);
+            bool nee;
+            Shadow sh;
+            const int step = shade<false>(S, path, hit, rec, depth, smp, rng, first, nee, sh, rays);
+            if (nee) {
+                bool ovf = false;
+                if (!occluded<false>(S, sh.o, sh.d, 0.001f, sh.t_max, stack, cnt, &ovf)) path.rad = path.rad + sh.value;
+                overflow |= ovf;
+            }
+            if (step == STEP_DONE) {
+                acc = acc + path.rad;
+                in_path = false;
+                ++s;
+            }
+        }
+
+        if (s >= spp) {
+            const float scale = 1.0f / float(spp);
+            float* out = B.out + __ldg(&B.scenes[sc].out_offset) + 3 * (size_t(height - 1 - pj) * width + pi);
+            out[0] = acc.x * scale;
+            out[1] = acc.y * scale;
+            out[2] = acc.z * scale;
+            has_pixel = false;
+            const uint32_t px = uint32_t(width) * uint32_t(height);
+            if (atomicAdd(B.done_pixels + sc, 1u) == px - 1) B.done_ns[sc] = global_ns();
+        }
+    }
+    unsigned long long total = rays;
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) total += __shfl_down_sync(0xffffffffu, total, off);
+    if (lane == 0 && B.rays) atomicAdd(B.rays, total);
+    if (__any_sync(0xffffffffu, overflow) && lane == 0) atomicOr(S0.status, PT_DEV_ERR_STACK);
+}
+
+template <int THREADS>
+int blocks_per_sm() {
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, batch_megakernel<THREADS>, THREADS, 0) != cudaSuccess) n = 1;
+    return n > 0 ? n : 1;
+}
+
+}  // namespace
+
+cudaError_t pt_launch_batch(const PtSceneDev& S, const PtBatchLaunch& b, int threads, int sms, cudaStream_t stream) {
+    switch (threads) {
+        case 64:
+            batch_megakernel<64><<<sms * blocks_per_sm<64>(), 64, 0, stream>>>(S, b);
+            break;
+        case 256:
+            batch_megakernel<256><<<sms * blocks_per_sm<256>(), 256, 0, stream>>>(S, b);
+            break;
+        default:
+            batch_megakernel<128><<<sms * blocks_per_sm<128>(), 128, 0, stream>>>(S, b);
+            break;
+    }
+    return cudaGetLastError();
+}

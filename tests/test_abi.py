@@ -42,7 +42,8 @@ def test_struct_sizes_match_c(built, tmp_path):
     """ctypes mirrors against sizeof/offsetof from a C compile of the header."""
     from photon_tracer_b200 import abi
     structs = ["pt_material", "pt_sphere", "pt_triangle", "pt_affine", "pt_bvh_node", "pt_bvh", "pt_mesh",
-               "pt_instance", "pt_scene_desc", "pt_scene_info", "pt_camera", "pt_settings", "pt_hit", "pt_gen_params"]
+               "pt_instance", "pt_scene_desc", "pt_scene_info", "pt_camera", "pt_settings", "pt_hit", "pt_gen_params",
+               "pt_batch_item", "pt_batch_info"]
     src = tmp_path / "sizes.c"
     src.write_text('#include <stdio.h>\n#include <stddef.h>\n#include "photon_cuda.h"\nint main(void){\n' +
                    "".join(f'printf("{s} %zu\\n", sizeof({s}));\n' for s in structs) +
@@ -138,3 +139,24 @@ def test_geometry_bridge_compiles_and_reports_no_device(built):
     res = subprocess.run([shim, "3"], capture_output=True, text=True, timeout=120)
     assert res.returncode == 3
     assert json.loads(res.stdout)["upload"] == 7
+
+
+def test_write_image_matches_reference(built, tmp_path):
+    """PFM and PPM bytes identical to the reference's write_image."""
+    from oracle.oracle import ref_available, ref_lib
+    rng = np.random.default_rng(4)
+    img = rng.uniform(-0.2, 1.6, (27, 48, 3)).astype(np.float32)
+    img[0, :4] = [[0, 0, 0], [1, 1, 1], [0.998, 0.999, 1.0], [4.0, 1e-9, 0.25]]
+    for ext in ("pfm", "ppm"):
+        mine = tmp_path / f"mine.{ext}"
+        built.write_image(str(mine), img)
+        data = mine.read_bytes()
+        if ext == "pfm":
+            head = b"PF\n48 27\n-1.0\n"
+            assert data.startswith(head)
+            back = np.frombuffer(data[len(head):], np.float32).reshape(27, 48, 3)[::-1]
+            assert np.array_equal(back, img)
+        if ref_available():
+            theirs = tmp_path / f"ref.{ext}"
+            assert ref_lib().ref_write_image(str(theirs).encode(), 48, 27, img.ctypes.data_as(C.c_void_p)) == 1
+            assert data == theirs.read_bytes()

@@ -264,6 +264,14 @@ pt_status pt_trace_closest_device(pt_scene* scene, const float* d_rays, size_t n
 pt_status pt_trace_any_device(pt_scene* scene, const float* d_rays, size_t n, float tmin, float tmax,
                               uint8_t* d_occluded, void* stream);
 
+/* Distance to the first surface along each pixel's centre ray (u = (i+0.5)/(W-1),
+ * v = (j+0.5)/(H-1) on include/camera.hpp:39-47), width*height floats, top row
+ * first, 0 where the ray leaves the scene: the depth guide of pt_denoise_unet.
+ * No reference counterpart (the reference's guides are albedo and normal,
+ * src/main.cpp:176-183). Device buffer, enqueued on stream. */
+pt_status pt_primary_depth_device(pt_scene* scene, const pt_camera* cam, int width, int height, float* d_depth,
+                                  void* stream);
+
 /* Traversal work counters for the algorithmic-bytes roofline: per ray, the
  * nodes visited, leaf-order entries read, triangles and spheres tested and
  * instances entered, summed over n rays (closest hit). Same traversal as
@@ -305,6 +313,54 @@ size_t pt_denoise_atrous_scratch_floats(int width, int height);
 pt_status pt_denoise_atrous_device_noalloc(int width, int height, const float* d_color, const float* d_albedo,
                                            const float* d_normal, const float* d_variance, float* d_out,
                                            void* stream);
+
+/* ---- learned denoiser (no reference counterpart) ---------------------------------
+ * A U-Net over 10 guide channels per pixel: radiance 3, albedo 3, normal 3 and
+ * depth 1 (the renderer's 7-float aux gives albedo and normal,
+ * pt_primary_depth_device the depth). Four levels of 32/64/96/128 channels, two
+ * 3x3 convolutions + ReLU per level, 2x2 max pooling, nearest 2x upsampling
+ * with skip concatenation, a final 3x3 convolution to log(1 + radiance).
+ * bfloat16 activations, float accumulation, float master weights, Adam.
+ *
+ * Parameters: 15 convolutions in forward order (32->32, 32->32, 32->64,
+ * 64->64, 64->96, 96->96, 96->128, 128->128, 224->96, 96->96, 160->64, 64->64,
+ * 96->32, 32->32, 32->16), each weights [Cout][3][3][Cin] then bias [Cout], as
+ * floats. The first layer's input channels 10..31 and the last layer's output
+ * channels 3..15 are padding.
+ *
+ * Batched tensors (forward, training): NHWC float, input 10 channels, target
+ * and output 3 (linear radiance); height and width multiples of 8. */
+typedef struct pt_unet pt_unet;
+pt_status pt_unet_create(uint64_t seed, pt_unet** out);
+pt_status pt_unet_destroy(pt_unet* net);
+size_t pt_unet_num_params(const pt_unet* net);
+pt_status pt_unet_get_params(const pt_unet* net, float* host_params);
+pt_status pt_unet_set_params(pt_unet* net, const float* host_params);
+/* 1 (default): convolutions with bfloat16 inputs run on the tensor cores where
+ * the shape allows; 0: on the CUDA cores only. */
+pt_status pt_unet_set_tensor_cores(pt_unet* net, int enable);
+/* Waits for the network's work on stream; PT_ERR_TIMEOUT if a tensor-core
+ * convolution gave up waiting for its operands since the last check. */
+pt_status pt_unet_sync(pt_unet* net, void* stream);
+pt_status pt_unet_forward(pt_unet* net, int batch, int height, int width, const float* d_input, float* d_output,
+                          void* stream);
+/* One Adam step (b1 0.9, b2 0.999, eps 1e-8) on the mean L1 distance between
+ * log(1 + output) and log(1 + target); *loss (may be NULL) gets that loss
+ * before the step. Synchronises stream. */
+pt_status pt_unet_train_step(pt_unet* net, int batch, int height, int width, const float* d_input,
+                             const float* d_target, float lr, float* loss, void* stream);
+/* The loss and its gradients without a step (synchronous, default stream):
+ * host_grads (NULL or pt_unet_num_params floats) in the parameter layout;
+ * host_input_grad (NULL or batch*height*width*32 floats) with respect to the
+ * network's padded input (log radiance, albedo, normal, log depth, zeros). */
+pt_status pt_unet_loss_grads(pt_unet* net, int batch, int height, int width, const float* d_input,
+                             const float* d_target, float* loss, float* host_grads, float* host_input_grad);
+/* Denoises one frame (any size; padded internally to multiples of 8 by
+ * repeating edge pixels): d_color 3 floats per pixel, d_aux the renderer's 7
+ * floats per pixel, d_depth 1 float per pixel, all top row first; d_out 3
+ * floats per pixel. Device buffers, enqueued on stream. */
+pt_status pt_denoise_unet(pt_unet* net, int width, int height, const float* d_color, const float* d_aux,
+                          const float* d_depth, float* d_out, void* stream);
 
 /* ---- ground truth and images ------------------------------------------------------- */
 /* Adds weight * d_frame[i] to d_sum[i] in FP64 (device buffers, enqueued on

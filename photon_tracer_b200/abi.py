@@ -156,6 +156,7 @@ PROTOTYPES = [
     ("pt_trace_any", ST, [P, P, SIZE, C.c_float, C.c_float, P]),
     ("pt_trace_closest_device", ST, [P, P, SIZE, C.c_float, C.c_float, P, P]),
     ("pt_trace_any_device", ST, [P, P, SIZE, C.c_float, C.c_float, P, P]),
+    ("pt_primary_depth_device", ST, [P, C.POINTER(pt_camera), C.c_int, C.c_int, P, P]),
     ("pt_trace_count", ST, [P, P, SIZE, C.c_float, C.c_float, C.POINTER(C.c_uint64)]),
     ("pt_bvh_build", ST, [P, C.c_uint32, C.POINTER(C.POINTER(pt_bvh_node)), C.POINTER(C.c_uint32),
                           C.POINTER(C.POINTER(C.c_uint32))]),
@@ -164,6 +165,17 @@ PROTOTYPES = [
     ("pt_denoise_atrous_device", ST, [C.c_int, C.c_int, P, P, P, P, P, P, P]),
     ("pt_denoise_atrous_scratch_floats", SIZE, [C.c_int, C.c_int]),
     ("pt_denoise_atrous_device_noalloc", ST, [C.c_int, C.c_int, P, P, P, P, P, P]),
+    ("pt_unet_create", ST, [C.c_uint64, C.POINTER(P)]),
+    ("pt_unet_destroy", ST, [P]),
+    ("pt_unet_num_params", SIZE, [P]),
+    ("pt_unet_get_params", ST, [P, P]),
+    ("pt_unet_set_params", ST, [P, P]),
+    ("pt_unet_set_tensor_cores", ST, [P, C.c_int]),
+    ("pt_unet_sync", ST, [P, P]),
+    ("pt_unet_forward", ST, [P, C.c_int, C.c_int, C.c_int, P, P, P]),
+    ("pt_unet_train_step", ST, [P, C.c_int, C.c_int, C.c_int, P, P, C.c_float, C.POINTER(C.c_float), P]),
+    ("pt_unet_loss_grads", ST, [P, C.c_int, C.c_int, C.c_int, P, P, C.POINTER(C.c_float), P, P]),
+    ("pt_denoise_unet", ST, [P, C.c_int, C.c_int, P, P, P, P, P]),
     ("pt_accumulate_pass", ST, [P, SIZE, C.c_double, P, P]),
     ("pt_write_image", ST, [C.c_char_p, C.c_int, C.c_int, P]),
     ("pt_to_display", C.c_uint8, [C.c_float]),

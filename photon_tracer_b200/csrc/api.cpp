@@ -423,6 +423,21 @@ pt_status pt_trace_any_device(pt_scene* s, const float* d_rays, size_t n, float 
     return PT_OK;
 }
 
+pt_status pt_primary_depth_device(pt_scene* s, const pt_camera* cam, int width, int height, float* d_depth,
+                                  void* stream) {
+    clear_error();
+    if (!s || !cam || !d_depth) return fail(PT_ERR_INVALID_ARG, "pt_primary_depth_device: null pointer");
+    if (width < 2 || height < 2) return fail(PT_ERR_INVALID_ARG, "pt_primary_depth_device: width and height must be >= 2");
+    if (pt_status e = use_device(s)) return e;
+    pt_settings st{};
+    st.width = width;
+    st.height = height;
+    const PtRenderParams p = make_params(cam, &st);
+    if (cudaError_t e = pt_launch_primary_depth(s->dev, p.cam, width, height, d_depth, static_cast<cudaStream_t>(stream)))
+        return cuda_fail(e, "primary_depth launch");
+    return PT_OK;
+}
+
 pt_status pt_trace_closest(pt_scene* s, const float* rays, size_t n, float tmin, float tmax, pt_hit* hits) {
     clear_error();
     if (!s || (n && (!rays || !hits))) return fail(PT_ERR_INVALID_ARG, "pt_trace_closest: null pointer");

@@ -44,3 +44,8 @@ cudaError_t pt_launch_trace_any(const PtSceneDev& scene, const float* rays, size
                                 uint8_t* occluded, cudaStream_t stream);
 cudaError_t pt_launch_trace_count(const PtSceneDev& scene, const float* rays, size_t n, float tmin, float tmax,
                                   unsigned long long* counts, cudaStream_t stream);
+
+// Distance to the first surface along each pixel's centre ray, top row first
+// (0 on a miss).
+cudaError_t pt_launch_primary_depth(const PtSceneDev& scene, const PtCamDev& cam, int width, int height, float* depth,
+                                    cudaStream_t stream);

@@ -82,6 +82,34 @@ __global__ void __launch_bounds__(128) trace_count_kernel(PtSceneDev S, const fl
     if (overflow) atomicOr(S.status, PT_DEV_ERR_STACK);
 }
 
+// Distance to the first surface along each pixel's centre ray (the depth
+// guide of the learned denoiser): u = (i + 0.5) / (W - 1), v = (j + 0.5) /
+// (H - 1) on the camera of include/camera.hpp:39-47, scanline j stored in
+// row H - 1 - j like the frame; 0 where the ray leaves the scene.
+__global__ void __launch_bounds__(128) primary_depth_kernel(PtSceneDev S, PtCamDev C, int width, int height,
+                                                             float* __restrict__ depth) {
+    StackEntry stack[PT_STACK_MAX];
+    bool overflow = false;
+    const V org = mk(C.origin[0], C.origin[1], C.origin[2]), llc = mk(C.llc[0], C.llc[1], C.llc[2]);
+    const V hor = mk(C.horizontal[0], C.horizontal[1], C.horizontal[2]);
+    const V ver = mk(C.vertical[0], C.vertical[1], C.vertical[2]);
+    const size_t n = size_t(width) * height;
+    for (size_t k = blockIdx.x * size_t(blockDim.x) + threadIdx.x; k < n; k += size_t(gridDim.x) * blockDim.x) {
+        const int i = int(k % width), j = int(k / width);
+        const float u = (float(i) + 0.5f) / float(width - 1), v = (float(j) + 0.5f) / float(height - 1);
+        const V d = llc + hor * u + ver * v - org;
+        float t = 1000.0f;
+        Hit h;
+        Counts cnt;
+        if (!closest<false>(S, org, d, 0.001f, t, h, stack, cnt)) {
+            overflow = true;
+            h.kind = PT_HIT_NONE;
+        }
+        depth[size_t(height - 1 - j) * width + i] = h.kind == PT_HIT_NONE ? 0.0f : t * sqrtf(dot(d, d));
+    }
+    if (overflow) atomicOr(S.status, PT_DEV_ERR_STACK);
+}
+
 int grid_for(size_t n, int threads) {
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
@@ -111,5 +139,13 @@ cudaError_t pt_launch_trace_count(const PtSceneDev& S, const float* rays, size_t
                                   unsigned long long* counts, cudaStream_t stream) {
     if (n == 0) return cudaSuccess;
     trace_count_kernel<<<grid_for(n, 128), 128, 0, stream>>>(S, rays, n, tmin, tmax, counts);
+    return cudaGetLastError();
+}
+
+cudaError_t pt_launch_primary_depth(const PtSceneDev& S, const PtCamDev& cam, int width, int height, float* depth,
+                                    cudaStream_t stream) {
+    const size_t n = size_t(width) * height;
+    if (n == 0) return cudaSuccess;
+    primary_depth_kernel<<<grid_for(n, 128), 128, 0, stream>>>(S, cam, width, height, depth);
     return cudaGetLastError();
 }

@@ -263,28 +263,99 @@ def run_batch_workload(args):
 
 def run_convergence_workload(args):
     """The headline study at 1920x1080: time to reach relMSE <= 0.01 against
-    FP64 ground truth for plain path tracing and for path tracing followed by
-    the a-trous filter, on held-out seeds of the random-spheres generator."""
+    FP64 ground truth for plain path tracing, for path tracing followed by the
+    a-trous filter, and for path tracing followed by the learned denoiser, on
+    held-out seeds (never used in training) of the scene generators."""
     import photon_tracer_b200 as pt
-    from photon_tracer_b200 import abi, metrics
+    from photon_tracer_b200 import denoiser, metrics
     w, h = 1920, 1080
+    net = denoiser.trained() if os.path.exists(denoiser.WEIGHTS) else None
     results = []
-    for seed in args.seeds:
-        g = pt.Generated(abi.PT_GEN_RANDOM_SPHERES, seed=seed)
-        cam = pt.camera_look_at((13, 2, 3), (0, 0, 0), 20.0, w / h)
-        scene = pt.Scene(g)
-        gt = metrics.GroundTruth(scene, cam, w, h, seed=seed, pass_spp=256)
-        t = time.perf_counter()
-        gt.add(max(1, args.gt_spp // 256))
-        gt_s = time.perf_counter() - t
-        truth = gt.image()
-        plain = metrics.time_to_error(scene, cam, w, h, truth, seed=seed, denoise=None)
-        den = metrics.time_to_error(scene, cam, w, h, truth, seed=seed, denoise="atrous", max_spp=1024)
-        results.append({"seed": seed, "gt_spp": gt.spp, "gt_s": round(gt_s, 2), "plain": plain, "atrous": den})
+    for kind in args.kinds:
+        for seed in args.seeds:
+            g, scene, cam = denoiser.scene_and_camera(kind, seed, w / h, jitter=False)
+            gt = metrics.GroundTruth(scene, cam, w, h, seed=seed, pass_spp=256)
+            t = time.perf_counter()
+            gt.add(max(1, args.gt_spp // 256))
+            gt_s = time.perf_counter() - t
+            truth = gt.image()
+            r = {"kind": kind, "seed": seed, "gt_spp": gt.spp, "gt_s": round(gt_s, 2)}
+            r["plain"] = metrics.time_to_error(scene, cam, w, h, truth, seed=seed, denoise=None,
+                                               max_spp=args.max_plain_spp)
+            r["atrous"] = metrics.time_to_error(scene, cam, w, h, truth, seed=seed, denoise="atrous", max_spp=1024)
+            if net is not None:
+                r["unet"] = metrics.time_to_error(scene, cam, w, h, truth, seed=seed, denoise="unet", max_spp=1024,
+                                                  net=net)
+            for leg in ("atrous", "unet"):
+                if leg in r and r[leg]["reached"] and r["plain"]["reached"]:
+                    r[f"speedup_{leg}"] = round(r["plain"]["ms"] / r[leg]["ms"], 2)
+            results.append(r)
+            print(json.dumps({"partial": {k: v for k, v in r.items() if k.startswith(("kind", "seed", "speedup"))}}),
+                  file=sys.stderr, flush=True)
     line = {"workload": "convergence", "metric": "1080p time-to-relMSE<=0.01, denoised vs plain GPU PT", "unit": "ms",
             "higher_is_better": False, "results": results,
             "note": "ground truth = FP64 per-pixel sums of gt_spp samples (numbered apart from the tested ones); "
-                    "times are GPU event times of render (+ filter)"}
+                    "times are GPU event times of render (+ depth guide + denoiser); unet = weights in "
+                    "photon_tracer_b200/weights, trained on other seeds"}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_unet_workload(args):
+    """The learned denoiser at 1920x1080: one frame through pt_denoise_unet
+    (guides in HBM), CUDA-event time over K frames, against the measured bf16
+    tensor peak; and one training step (16 crops of 128^2) through
+    pt_unet_train_step."""
+    import torch
+    from photon_tracer_b200 import denoiser
+    from photon_tracer_b200.unet import UNet, conv_flops
+    w, h = 1920, 1080
+    net = denoiser.trained() if os.path.exists(denoiser.WEIGHTS) else UNet(seed=1)
+    gen = torch.Generator(device="cuda").manual_seed(SEED)
+    color = torch.rand((h, w, 3), device="cuda", generator=gen)
+    aux = torch.rand((h, w, 7), device="cuda", generator=gen)
+    depth = torch.rand((h, w), device="cuda", generator=gen)
+    flush = torch.empty(64 << 20, dtype=torch.float32, device="cuda")
+    for _ in range(args.warmup):
+        net.denoise(color, aux, depth)
+    net.sync()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    for a, b in ev:
+        flush.zero_()
+        a.record()
+        net.denoise(color, aux, depth)
+        b.record()
+    net.sync()
+    ms = sum(a.elapsed_time(b) for a, b in ev) / args.steps
+    flops = conv_flops(1, (h + 7) // 8 * 8, (w + 7) // 8 * 8)
+    try:
+        with open(PEAKS) as f:
+            peak, kind = float(json.load(f)["bf16_tflops"]), "measured"
+    except Exception:
+        peak, kind = 1590.0, "fallback"
+    tflops = flops / ms / 1e9
+    # one training step
+    x = torch.rand((16, 128, 128, 10), device="cuda", generator=gen)
+    t = torch.rand((16, 128, 128, 3), device="cuda", generator=gen)
+    train_net = UNet(seed=2)
+    for _ in range(3):
+        train_net.train_step(x, t, 1e-4)
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    for _ in range(10):
+        train_net.train_step(x, t, 1e-4)
+    b.record()
+    torch.cuda.synchronize()
+    train_ms = a.elapsed_time(b) / 10
+    line = {"workload": "unet", "metric": "U-Net denoise of one 1920x1080 frame", "value": round(ms, 3), "unit": "ms",
+            "higher_is_better": False, "steps": args.steps, "warmup": args.warmup, "dtype": "bf16 (fp32 accumulate)",
+            "config": {"workload": "U-Net 10->32/64/96/128, 15 3x3 convs, 1920x1080 (padded to 1920x1080)",
+                       "l2": "flushed (256 MB write) between frames"},
+            "roofline": {"bound": "tensor", "achieved": round(tflops, 1), "peak": peak, "unit": "TFLOP/s",
+                         "frac": round(tflops / peak, 4), "peak_kind": kind,
+                         "flops_per_frame": flops, "note": "2*9*Cin*Cout*pixels over the 15 convs as computed "
+                                                           "(input padded to 32 channels, output to 16)"},
+            "train_step_ms": round(train_ms, 3), "train_batch": "16 x 128 x 128"}
     print(json.dumps(line), flush=True)
     return 0
 
@@ -329,10 +400,14 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--mode", default="mega", choices=["mega", "wave"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="room", choices=["room", "batch", "convergence", "instances", "spheres"],
+    ap.add_argument("--workload", default="room",
+                    choices=["room", "batch", "convergence", "unet", "instances", "spheres"],
                     help="room: the headline line (config 1); the others print their own JSON line")
     ap.add_argument("--seeds", type=int, nargs="+", default=[1001, 1002])
+    ap.add_argument("--kinds", nargs="+", default=["spheres", "room", "instances"],
+                    help="convergence: scene generators (random spheres, room mesh, instancing)")
     ap.add_argument("--gt-spp", type=int, default=4096)
+    ap.add_argument("--max-plain-spp", type=int, default=4096)
     ap.add_argument("--profile-case", action="store_true",
                     help="the case profiles are taken on: 1024x1024 at 4 spp, 3 frames, no baselines")
     args = ap.parse_args()
@@ -355,6 +430,8 @@ def main():
             return run_batch_workload(args)
         if args.workload == "convergence":
             return run_convergence_workload(args)
+        if args.workload == "unet":
+            return run_unet_workload(args)
         if args.workload == "instances":
             return run_scene_workload(args, _abi.PT_GEN_INSTANCES, "instances")
         return run_scene_workload(args, _abi.PT_GEN_RANDOM_SPHERES, "spheres")

@@ -81,6 +81,7 @@ struct pt_unet {
     DevBuf pool[3];      // p0, p1, p2
     DevBuf cat[3];       // u0, u1, u2
     DevBuf gact[16];     // gradients of x0, a0..a13, out
+    DevBuf g16;          // bf16 copy of the latest ReLU-masked gradient (tensor-core backward)
     DevBuf gpool[3], gcat[3];
     DevBuf loss;
     DevBuf status;
@@ -106,6 +107,12 @@ cudaError_t ensure_workspace(pt_unet* n, int B, int H, int W) {
         e = n->act[i].ensure(px * c * (i == 15 ? 4 : 2));
         if (!e) e = n->gact[i].ensure(px * c * 4);
     }
+    size_t g16_elems = 0;
+    for (int i = 1; i < 15; ++i) {
+        const size_t c = size_t(pixels_at(n, act_level(i))) * act_channels(i);
+        g16_elems = c > g16_elems ? c : g16_elems;
+    }
+    if (!e) e = n->g16.ensure(g16_elems * 2);
     const int pool_c[3] = {32, 64, 96}, cat_c[3] = {96, 160, 224};
     for (int l = 0; l < 3 && !e; ++l) {
         const size_t pp = size_t(pixels_at(n, l + 1)), pc = size_t(pixels_at(n, l));
@@ -186,54 +193,73 @@ cudaError_t backward(pt_unet* n, cudaStream_t st) {
     auto g = [&](int i) { return n->gact[i].as<float>(); };
     // One convolution's backward: weight gradients from its input and output
     // gradient, and the input gradient through the flip-transposed weights.
-    auto conv_back = [&](int l, const __nv_bfloat16* in, const float* gout, float* gin) -> cudaError_t {
+    // With tensor cores on, a layer's output gradient is also rounded to bf16
+    // (the copy relu_back, or to_bf16 for the last layer, leaves in g16): its
+    // weight gradient is a tcgen05 GEMM over pixels of that copy and the
+    // layer input, and its input gradient the tcgen05 convolution of that
+    // copy with the flip-transposed weights. Tensor cores off: the float
+    // gradient on CUDA cores.
+    __nv_bfloat16* g16 = n->use_tc ? n->g16.as<__nv_bfloat16>() : nullptr;
+    auto conv_back = [&](int l, const __nv_bfloat16* in, const float* gout, bool gout16, float* gin) -> cudaError_t {
         const LayerDef& L = kLayers[l];
         const unet::ConvShape s{B, H >> L.level, W >> L.level, L.cin, L.cout};
-        cudaError_t r = unet::conv_wgrad(s, in, gout, G + n->w_off[l], G + n->b_off[l], st);
+        cudaError_t r = cudaErrorNotSupported;
+        if (gout16 && g16) {
+            r = unet::conv_wgrad_tc(s, in, g16, G + n->w_off[l], n->status.as<unsigned int>(), st);
+            if (!r) r = unet::bias_grad(pixels_at(n, L.level), L.cout, gout, G + n->b_off[l], st);
+        }
+        if (r == cudaErrorNotSupported) r = unet::conv_wgrad(s, in, gout, G + n->w_off[l], G + n->b_off[l], st);
         if (r || !gin) return r;
         const unet::ConvShape t{B, H >> L.level, W >> L.level, L.cout, L.cin};
-        return unet::conv_fwd(t, gout, true, n->wt16.as<__nv_bfloat16>() + n->w_off[l], nullptr, false, gin, true,
-                              L.cin, 0, st);
+        const __nv_bfloat16* wt = n->wt16.as<__nv_bfloat16>() + n->w_off[l];
+        if (gout16 && g16) {
+            r = unet::conv_fwd_tc(t, g16, wt, nullptr, false, gin, true, L.cin, 0, n->status.as<unsigned int>(), st);
+            if (r != cudaErrorNotSupported) return r;
+        }
+        return unet::conv_fwd(t, gout, true, wt, nullptr, false, gin, true, L.cin, 0, st);
     };
-    auto relu_back = [&](int i) { return unet::relu_grad(pixels_at(n, act_level(i)) * act_channels(i), bf(i), g(i), nullptr, st); };
-    TRY(conv_back(14, bf(14), g(15), g(14)));
+    auto relu_back = [&](int i) {
+        return unet::relu_grad(pixels_at(n, act_level(i)) * act_channels(i), bf(i), g(i), g16, st);
+    };
+    if (g16) TRY(unet::to_bf16(pixels_at(n, 0) * kOutStride, g(15), g16, st));
+    TRY(conv_back(14, bf(14), g(15), true, g(14)));
     TRY(relu_back(14));
-    TRY(conv_back(13, bf(13), g(14), g(13)));
+    TRY(conv_back(13, bf(13), g(14), true, g(13)));
     TRY(relu_back(13));
-    TRY(conv_back(12, n->cat[0].as<__nv_bfloat16>(), g(13), n->gcat[0].as<float>()));
+    TRY(conv_back(12, n->cat[0].as<__nv_bfloat16>(), g(13), true, n->gcat[0].as<float>()));
     TRY(unet::up_bwd(B, H / 2, W / 2, 64, n->gcat[0].as<float>(), 96, 0, g(12), st));
     TRY(unet::add_channels(pixels_at(n, 0), 32, n->gcat[0].as<float>(), 96, 64, g(2), st));
     TRY(relu_back(12));
-    TRY(conv_back(11, bf(11), g(12), g(11)));
+    TRY(conv_back(11, bf(11), g(12), true, g(11)));
     TRY(relu_back(11));
-    TRY(conv_back(10, n->cat[1].as<__nv_bfloat16>(), g(11), n->gcat[1].as<float>()));
+    TRY(conv_back(10, n->cat[1].as<__nv_bfloat16>(), g(11), true, n->gcat[1].as<float>()));
     TRY(unet::up_bwd(B, H / 4, W / 4, 96, n->gcat[1].as<float>(), 160, 0, g(10), st));
     TRY(unet::add_channels(pixels_at(n, 1), 64, n->gcat[1].as<float>(), 160, 96, g(4), st));
     TRY(relu_back(10));
-    TRY(conv_back(9, bf(9), g(10), g(9)));
+    TRY(conv_back(9, bf(9), g(10), true, g(9)));
     TRY(relu_back(9));
-    TRY(conv_back(8, n->cat[2].as<__nv_bfloat16>(), g(9), n->gcat[2].as<float>()));
+    TRY(conv_back(8, n->cat[2].as<__nv_bfloat16>(), g(9), true, n->gcat[2].as<float>()));
     TRY(unet::up_bwd(B, H / 8, W / 8, 128, n->gcat[2].as<float>(), 224, 0, g(8), st));
     TRY(unet::add_channels(pixels_at(n, 2), 96, n->gcat[2].as<float>(), 224, 128, g(6), st));
     TRY(relu_back(8));
-    TRY(conv_back(7, bf(7), g(8), g(7)));
+    TRY(conv_back(7, bf(7), g(8), true, g(7)));
     TRY(relu_back(7));
-    TRY(conv_back(6, n->pool[2].as<__nv_bfloat16>(), g(7), n->gpool[2].as<float>()));
+    TRY(conv_back(6, n->pool[2].as<__nv_bfloat16>(), g(7), true, n->gpool[2].as<float>()));
     TRY(unet::pool_bwd(B, H / 4, W / 4, 96, bf(6), n->pool[2].as<__nv_bfloat16>(), n->gpool[2].as<float>(), g(6), st));
     TRY(relu_back(6));
-    TRY(conv_back(5, bf(5), g(6), g(5)));
+    TRY(conv_back(5, bf(5), g(6), true, g(5)));
     TRY(relu_back(5));
-    TRY(conv_back(4, n->pool[1].as<__nv_bfloat16>(), g(5), n->gpool[1].as<float>()));
+    TRY(conv_back(4, n->pool[1].as<__nv_bfloat16>(), g(5), true, n->gpool[1].as<float>()));
     TRY(unet::pool_bwd(B, H / 2, W / 2, 64, bf(4), n->pool[1].as<__nv_bfloat16>(), n->gpool[1].as<float>(), g(4), st));
     TRY(relu_back(4));
-    TRY(conv_back(3, bf(3), g(4), g(3)));
+    TRY(conv_back(3, bf(3), g(4), true, g(3)));
     TRY(relu_back(3));
-    TRY(conv_back(2, n->pool[0].as<__nv_bfloat16>(), g(3), n->gpool[0].as<float>()));
+    TRY(conv_back(2, n->pool[0].as<__nv_bfloat16>(), g(3), true, n->gpool[0].as<float>()));
     TRY(unet::pool_bwd(B, H, W, 32, bf(2), n->pool[0].as<__nv_bfloat16>(), n->gpool[0].as<float>(), g(2), st));
     TRY(relu_back(2));
-    TRY(conv_back(1, bf(1), g(2), g(1)));
+    TRY(conv_back(1, bf(1), g(2), true, g(1)));
     TRY(relu_back(1));
-    TRY(conv_back(0, bf(0), g(1), g(0)));
+    TRY(conv_back(0, bf(0), g(1), true, g(0)));
 #undef TRY
     return cudaSuccess;
 }

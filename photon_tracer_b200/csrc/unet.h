@@ -16,6 +16,8 @@ cudaError_t conv_fwd(const ConvShape& s, const void* in, bool in_f32, const __nv
 // dw += d loss / d w, db += d loss / d bias, from the layer input and the gradient of its output.
 cudaError_t conv_wgrad(const ConvShape& s, const __nv_bfloat16* in, const float* dout, float* dw, float* db,
                        cudaStream_t st);
+// db[c] += sum over pixels of g[p][c], g NHWC float with C <= 256 channels.
+cudaError_t bias_grad(long pixels, int C, const float* g, float* db, cudaStream_t st);
 cudaError_t flip_transpose(int Cin, int Cout, const __nv_bfloat16* w, __nv_bfloat16* wt, cudaStream_t st);
 cudaError_t relu_grad(long n, const __nv_bfloat16* y, float* g, __nv_bfloat16* g16, cudaStream_t st);
 cudaError_t to_bf16(long n, const float* g, __nv_bfloat16* g16, cudaStream_t st);
@@ -46,5 +48,12 @@ cudaError_t f32_to_bf16(long n, const float* a, __nv_bfloat16* b, cudaStream_t s
 cudaError_t conv_fwd_tc(const ConvShape& s, const __nv_bfloat16* in, const __nv_bfloat16* w, const float* bias,
                         bool relu, void* out, bool out_f32, int out_stride, int out_offset, unsigned int* status,
                         cudaStream_t st);
+
+// Tensor-core weight gradient (tcgen05, MN-major operands): dw += d loss /
+// d w from the layer input and the bf16 gradient of its output (Cout <= 128,
+// Cin <= 256, both multiples of 8), float atomics. cudaErrorNotSupported for
+// other shapes, which then run on conv_wgrad.
+cudaError_t conv_wgrad_tc(const ConvShape& s, const __nv_bfloat16* in, const __nv_bfloat16* dout, float* dw,
+                          unsigned int* status, cudaStream_t st);
 
 }  // namespace unet

@@ -132,6 +132,26 @@ __global__ void __launch_bounds__(256) conv_wgrad_kernel(int B, int H, int W, in
     if (db && tap == 0 && ci0 == 0 && t < kCoTile && co0 + t < Cout) atomicAdd(&db[co0 + t], bacc);
 }
 
+// db[c] += sum over pixels of g[p][c] (C <= 256): R = 256 / C rows of
+// threads per block stride over the block's pixels, then one row sums.
+__global__ void __launch_bounds__(256) bias_grad_kernel(long pixels, int C, const float* __restrict__ g,
+                                                        float* __restrict__ db, long px_per_block) {
+    __shared__ float part[256];
+    const int R = 256 / C;
+    const int t = threadIdx.x, c = t % C, r = t / C;
+    const long p0 = long(blockIdx.x) * px_per_block;
+    const long p1 = p0 + px_per_block < pixels ? p0 + px_per_block : pixels;
+    float acc = 0.0f;
+    if (r < R)
+        for (long p = p0 + r; p < p1; p += R) acc += g[p * C + c];
+    part[t] = acc;
+    __syncthreads();
+    if (r == 0) {
+        for (int k = 1; k < R; ++k) acc += part[k * C + c];
+        atomicAdd(db + c, acc);
+    }
+}
+
 // w_t[ci][tap][co] = w[co][8 - tap][ci]: the weights of the transposed
 // convolution that carries gradients back to a layer's input.
 __global__ void flip_transpose_kernel(int Cin, int Cout, const __nv_bfloat16* __restrict__ w,
@@ -382,6 +402,14 @@ cudaError_t conv_wgrad(const ConvShape& s, const __nv_bfloat16* in, const float*
     splits = int((P + per - 1) / per);
     const dim3 grid(unsigned(9 * ci_tiles), unsigned(co_tiles), unsigned(splits));
     conv_wgrad_kernel<<<grid, 256, 0, st>>>(s.B, s.H, s.W, s.Cin, s.Cout, in, dout, dw, db, per);
+    return cudaGetLastError();
+}
+
+cudaError_t bias_grad(long pixels, int C, const float* g, float* db, cudaStream_t st) {
+    if (C < 1 || C > 256) return cudaErrorInvalidValue;
+    const long per = 4096;
+    const long blocks = (pixels + per - 1) / per;
+    bias_grad_kernel<<<unsigned(blocks > 0 ? blocks : 1), 256, 0, st>>>(pixels, C, g, db, per);
     return cudaGetLastError();
 }
 

@@ -9,7 +9,8 @@
 //      the [Cout][3][3][Cin] bf16 weights -- Cout rows of 64 bytes.
 // Both land K-major with the 64-byte swizzle; two MMAs of K = 16 consume a
 // step. One warp issues TMA, one thread issues MMAs, four warps drain the
-// accumulator (bias, ReLU, bf16 or float) straight to global memory.
+// accumulator (bias, ReLU, bf16 or float) straight to global memory. CTAs
+// are persistent over tiles with two TMEM accumulators.
 //
 // Every wait on an mbarrier is bounded (1 s); on expiry the kernel sets bit
 // 0 of *status, lets the copies it issued land, frees its TMEM and returns.
@@ -132,10 +133,28 @@ __device__ __forceinline__ void tmem_ld16(uint32_t addr, float (&v)[16]) {
     for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
 
+__device__ __forceinline__ void bar_arrive(uint32_t bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+
+struct TileGrid {
+    int tiles_x, tiles_y, n;
+    __device__ void origin(int t, int& x0, int& y0, int& b) const {
+        x0 = (t % tiles_x) * kTileX;
+        t /= tiles_x;
+        y0 = (t % tiles_y) * kTileY;
+        b = t / tiles_y;
+    }
+};
+
+// Persistent: CTA c takes tiles c, c + gridDim.x, ... Two accumulators in
+// TMEM (columns from 0 and from half the allocation, a power of two >= 2N)
+// let the epilogue of one tile overlap the MMAs of the next; the TMA
+// producer runs ahead across tile boundaries.
 template <bool OUT_F32>
 __global__ void __launch_bounds__(kThreads) conv_tc_kernel(const __grid_constant__ CUtensorMap tm_in,
-                                                           const __grid_constant__ CUtensorMap tm_w, int H, int W,
-                                                           int Cin, int N, int tmem_cols,
+                                                           const __grid_constant__ CUtensorMap tm_w, int B, int H,
+                                                           int W, int Cin, int N, int tmem_cols,
                                                            const float* __restrict__ bias, int relu,
                                                            void* __restrict__ out, int out_stride, int out_offset,
                                                            unsigned int* __restrict__ status) {
@@ -144,18 +163,18 @@ __global__ void __launch_bounds__(kThreads) conv_tc_kernel(const __grid_constant
     const uint32_t b_bytes = uint32_t(N) * kKc * 2;
     uint8_t* sa = smem;
     uint8_t* sb = smem + kStages * kABytes;
-    uint64_t* bars = reinterpret_cast<uint64_t*>(sb + kStages * b_bytes);  // full[S], empty[S], done
-    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * kStages + 1);
+    // full[S], empty[S], acc_full[2], acc_empty[2]
+    uint64_t* bars = reinterpret_cast<uint64_t*>(sb + kStages * b_bytes);
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * kStages + 4);
     volatile int* abort = reinterpret_cast<volatile int*>(tmem_slot + 1);
-    const uint32_t full0 = smem_u32(bars), empty0 = smem_u32(bars + kStages), done = smem_u32(bars + 2 * kStages);
+    const uint32_t full0 = smem_u32(bars), empty0 = smem_u32(bars + kStages);
+    const uint32_t acc_full0 = smem_u32(bars + 2 * kStages), acc_empty0 = smem_u32(bars + 2 * kStages + 2);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int tiles_x = (W + kTileX - 1) / kTileX, tiles_y = (H + kTileY - 1) / kTileY;
-    int t = blockIdx.x;
-    const int x0 = (t % tiles_x) * kTileX;
-    t /= tiles_x;
-    const int y0 = (t % tiles_y) * kTileY;
-    const int b = t / tiles_y;
+    TileGrid grid;
+    grid.tiles_x = (W + kTileX - 1) / kTileX;
+    grid.tiles_y = (H + kTileY - 1) / kTileY;
+    grid.n = grid.tiles_x * grid.tiles_y * B;
     const int chunks = Cin / kKc, iters = 9 * chunks;
 
     if (threadIdx.x == 0) {
@@ -163,7 +182,10 @@ __global__ void __launch_bounds__(kThreads) conv_tc_kernel(const __grid_constant
             bar_init(full0 + 8 * s, 1);
             bar_init(empty0 + 8 * s, 1);
         }
-        bar_init(done, 1);
+        for (int a = 0; a < 2; ++a) {
+            bar_init(acc_full0 + 8 * a, 1);
+            bar_init(acc_empty0 + 8 * a, 4);  // one arrival per epilogue warp
+        }
         *abort = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
@@ -183,20 +205,25 @@ __global__ void __launch_bounds__(kThreads) conv_tc_kernel(const __grid_constant
         if (lane == 0) {
             asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&tm_in)) : "memory");
             asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&tm_w)) : "memory");
-            int it = 0;
-            for (; it < iters; ++it) {
-                const int s = it % kStages;
-                if (it >= kStages && !wait_bar(empty0 + 8 * s, ((it / kStages) - 1) & 1, abort)) {
-                    ok = false;
-                    break;
+            int g = 0;  // k steps issued so far, over all of this CTA's tiles
+            for (int t = blockIdx.x; t < grid.n && ok; t += gridDim.x) {
+                int x0, y0, b;
+                grid.origin(t, x0, y0, b);
+                for (int it = 0; it < iters; ++it, ++g) {
+                    const int s = g % kStages;
+                    if (g >= kStages && !wait_bar(empty0 + 8 * s, ((g / kStages) - 1) & 1, abort)) {
+                        ok = false;
+                        break;
+                    }
+                    const int tap = it / chunks, c0 = (it - tap * chunks) * kKc;
+                    bar_expect_tx(full0 + 8 * s, kABytes + b_bytes);
+                    tma_load_4d(smem_u32(sa + s * kABytes), &tm_in, c0, x0 + tap % 3 - 1, y0 + tap / 3 - 1, b,
+                                full0 + 8 * s);
+                    tma_load_3d(smem_u32(sb + s * b_bytes), &tm_w, c0, tap, 0, full0 + 8 * s);
                 }
-                const int tap = it / chunks, c0 = (it - tap * chunks) * kKc;
-                bar_expect_tx(full0 + 8 * s, kABytes + b_bytes);
-                tma_load_4d(smem_u32(sa + s * kABytes), &tm_in, c0, x0 + tap % 3 - 1, y0 + tap / 3 - 1, b, full0 + 8 * s);
-                tma_load_3d(smem_u32(sb + s * b_bytes), &tm_w, c0, tap, 0, full0 + 8 * s);
             }
             // The copies issued into each stage have landed before the CTA can exit.
-            for (int k = it > kStages ? it - kStages : 0; k < it; ++k)
+            for (int k = g > kStages ? g - kStages : 0; k < g; ++k)
                 if (!wait_bar(full0 + 8 * (k % kStages), (k / kStages) & 1, nullptr)) ok = false;
         }
     } else if (warp == 1) {
@@ -205,57 +232,78 @@ __global__ void __launch_bounds__(kThreads) conv_tc_kernel(const __grid_constant
             // A and B bf16 (bits 7-9, 10-12 = 1), both K-major, N >> 3 at bit
             // 17, M >> 4 at bit 24.
             const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | (uint32_t(N >> 3) << 17) | (uint32_t(kM >> 4) << 24);
-            for (int it = 0; it < iters; ++it) {
-                const int s = it % kStages;
-                if (!wait_bar(full0 + 8 * s, (it / kStages) & 1, abort)) {
+            int g = 0, i = 0;
+            for (int t = blockIdx.x; t < grid.n && ok; t += gridDim.x, ++i) {
+                const int a = i & 1;
+                if (i >= 2 && !wait_bar(acc_empty0 + 8 * a, ((i >> 1) - 1) & 1, abort)) {
                     ok = false;
                     break;
                 }
                 fence_after();
-                const uint64_t ad = sw64_desc(smem_u32(sa + s * kABytes)), bd = sw64_desc(smem_u32(sb + s * b_bytes));
+                const uint32_t d = tmem + uint32_t(a * (tmem_cols / 2));
+                for (int it = 0; it < iters; ++it, ++g) {
+                    const int s = g % kStages;
+                    if (!wait_bar(full0 + 8 * s, (g / kStages) & 1, abort)) {
+                        ok = false;
+                        break;
+                    }
+                    fence_after();
+                    const uint64_t ad = sw64_desc(smem_u32(sa + s * kABytes));
+                    const uint64_t bd = sw64_desc(smem_u32(sb + s * b_bytes));
 #pragma unroll
-                for (int k = 0; k < kKc / 16; ++k)  // K = 16 per MMA: +32 bytes along the row
-                    mma_bf16(tmem, ad + uint64_t(2 * k), bd + uint64_t(2 * k), idesc, (it | k) != 0);
-                mma_commit(empty0 + 8 * s);
+                    for (int k = 0; k < kKc / 16; ++k)  // K = 16 per MMA: +32 bytes along the row
+                        mma_bf16(d, ad + uint64_t(2 * k), bd + uint64_t(2 * k), idesc, (it | k) != 0);
+                    mma_commit(empty0 + 8 * s);
+                }
+                mma_commit(acc_full0 + 8 * a);
             }
-            mma_commit(done);
         }
     } else {
         const int q = warp & 3;  // the TMEM lane quarter this warp may read
         const int m = q * 32 + lane;
-        const int px = x0 + (m % kTileX), py = y0 + (m / kTileX);
-        const bool valid = px < W && py < H;
-        const bool got = __all_sync(0xffffffffu, wait_bar(done, 0, abort));
-        if (got) {
+        int i = 0;
+        for (int t = blockIdx.x; t < grid.n; t += gridDim.x, ++i) {
+            const int a = i & 1;
+            if (!__all_sync(0xffffffffu, wait_bar(acc_full0 + 8 * a, (i >> 1) & 1, abort))) {
+                ok = false;
+                break;
+            }
             fence_after();
+            int x0, y0, b;
+            grid.origin(t, x0, y0, b);
+            const int px = x0 + (m % kTileX), py = y0 + (m / kTileX);
+            const bool valid = px < W && py < H;
             const size_t pix = (size_t(b) * H + (valid ? py : 0)) * W + (valid ? px : 0);
             for (int c = 0; c < N; c += 16) {
                 float v[16];
-                tmem_ld16(tmem + (uint32_t(q * 32) << 16) + uint32_t(c), v);
+                tmem_ld16(tmem + (uint32_t(q * 32) << 16) + uint32_t(a * (tmem_cols / 2) + c), v);
                 if (!valid) continue;
 #pragma unroll
-                for (int i = 0; i < 16; ++i) {
-                    v[i] += bias ? bias[c + i] : 0.0f;
-                    if (relu) v[i] = fmaxf(v[i], 0.0f);
+                for (int j = 0; j < 16; ++j) {
+                    v[j] += bias ? bias[c + j] : 0.0f;
+                    if (relu) v[j] = fmaxf(v[j], 0.0f);
                 }
                 if (OUT_F32) {
                     float4* dst = reinterpret_cast<float4*>(static_cast<float*>(out) + pix * out_stride + out_offset + c);
 #pragma unroll
-                    for (int i = 0; i < 4; ++i) dst[i] = make_float4(v[4 * i], v[4 * i + 1], v[4 * i + 2], v[4 * i + 3]);
+                    for (int j = 0; j < 4; ++j) dst[j] = make_float4(v[4 * j], v[4 * j + 1], v[4 * j + 2], v[4 * j + 3]);
                 } else {
                     uint32_t w[8];
 #pragma unroll
-                    for (int i = 0; i < 8; ++i) {
-                        const __nv_bfloat162 h = __floats2bfloat162_rn(v[2 * i], v[2 * i + 1]);
-                        w[i] = *reinterpret_cast<const uint32_t*>(&h);
+                    for (int j = 0; j < 8; ++j) {
+                        const __nv_bfloat162 h = __floats2bfloat162_rn(v[2 * j], v[2 * j + 1]);
+                        w[j] = *reinterpret_cast<const uint32_t*>(&h);
                     }
-                    uint4* dst = reinterpret_cast<uint4*>(static_cast<__nv_bfloat16*>(out) + pix * out_stride + out_offset + c);
+                    uint4* dst =
+                        reinterpret_cast<uint4*>(static_cast<__nv_bfloat16*>(out) + pix * out_stride + out_offset + c);
                     dst[0] = make_uint4(w[0], w[1], w[2], w[3]);
                     dst[1] = make_uint4(w[4], w[5], w[6], w[7]);
                 }
             }
-        } else {
-            ok = false;
+            // This warp's reads of the accumulator are done: the MMA warp may reuse it.
+            fence_before();
+            __syncwarp();
+            if (lane == 0) bar_arrive(acc_empty0 + 8 * a);
         }
     }
 
@@ -284,7 +332,166 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
     return fn;
 }
 
-size_t smem_bytes(int N) { return 1024 + kStages * (kABytes + size_t(N) * kKc * 2) + (2 * kStages + 1) * 8 + 8; }
+size_t smem_bytes(int N) { return 1024 + kStages * (kABytes + size_t(N) * kKc * 2) + (2 * kStages + 4) * 8 + 8; }
+
+// Resident CTAs per SM for this N (shared memory and TMEM columns), and SMs.
+int grid_size(int N, int cols, size_t smem, const void* fn) {
+    static int sms[64] = {0};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 64) dev = 0;
+    if (!sms[dev]) {
+        int n = 0;
+        cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+        sms[dev] = n > 0 ? n : 1;
+    }
+    int per_sm = 1;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kThreads, smem) != cudaSuccess || per_sm < 1)
+        per_sm = 1;
+    const int by_tmem = 512 / cols;
+    return sms[dev] * (per_sm < by_tmem ? per_sm : by_tmem);
+}
+
+// ---- weight gradient -------------------------------------------------------
+// dW[co][tap][ci] = sum over pixels p of dY[p][co] * X[p + offset(tap)][ci]:
+// per tap a GEMM with M = Cout (padded to 128), N = Cin (padded to a
+// multiple of 64), K = pixels. A K step is a 16 x 4 pixel box: dY unshifted
+// and X shifted by the tap (zeros outside the image), both channel-contiguous
+// -- MN-major operands, 128-byte swizzle, one 64-channel TMA box per 64
+// rows of M or N. A CTA reduces one tap over a range of pixel boxes in TMEM
+// and adds its partial sums to dW with float atomics.
+constexpr int kWgBoxX = 16, kWgBoxY = 4, kWgK = kWgBoxX * kWgBoxY;  // 64 pixels per K step
+constexpr int kWgStages = 4;
+constexpr uint32_t kWgBox = kWgK * 64 * 2;  // one 64-channel box: 8 KB
+
+// UMMA descriptor of an MN-major operand with the 128-byte swizzle: 64
+// elements of M or N per 128-byte row, one row per K index; 8-row groups
+// 1024 bytes apart (stride byte offset), 64-element blocks of M or N one
+// 8 KB box apart (leading byte offset), descriptor version 1.
+__device__ __forceinline__ uint64_t mn_sw128_desc(uint32_t addr) {
+    return uint64_t((addr >> 4) & 0x3fff) | (uint64_t(kWgBox >> 4) << 16) | (uint64_t(1024 >> 4) << 32) |
+           (uint64_t(1) << 46) | (uint64_t(2) << 61);
+}
+
+__global__ void __launch_bounds__(kThreads) wgrad_tc_kernel(const __grid_constant__ CUtensorMap tm_dy,
+                                                            const __grid_constant__ CUtensorMap tm_x, int B, int H,
+                                                            int W, int Cin, int Cout, int N, int tmem_cols, int splits,
+                                                            float* __restrict__ dw, unsigned int* __restrict__ status) {
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    const int nb = N / 64;  // X boxes per stage
+    const uint32_t stage_bytes = (2 + nb) * kWgBox;
+    uint64_t* bars = reinterpret_cast<uint64_t*>(smem + kWgStages * stage_bytes);  // full[S], empty[S], done
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * kWgStages + 1);
+    volatile int* abort = reinterpret_cast<volatile int*>(tmem_slot + 1);
+    const uint32_t full0 = smem_u32(bars), empty0 = smem_u32(bars + kWgStages), done = smem_u32(bars + 2 * kWgStages);
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int tap = blockIdx.x % 9, split = blockIdx.x / 9;
+    const int bx = (W + kWgBoxX - 1) / kWgBoxX, by = (H + kWgBoxY - 1) / kWgBoxY;
+    const long boxes = long(bx) * by * B;
+    const long k0 = boxes * split / splits, k1 = boxes * (split + 1) / splits;
+    const int iters = int(k1 - k0);
+    const int dy = tap / 3 - 1, dx = tap % 3 - 1;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < kWgStages; ++s) {
+            bar_init(full0 + 8 * s, 1);
+            bar_init(empty0 + 8 * s, 1);
+        }
+        bar_init(done, 1);
+        *abort = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                     "r"(tmem_cols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    fence_before();
+    __syncthreads();
+    fence_after();
+    const uint32_t tmem = *tmem_slot;
+    bool ok = true;
+
+    if (warp == 0) {
+        if (lane == 0) {
+            asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&tm_dy)) : "memory");
+            asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&tm_x)) : "memory");
+            int it = 0;
+            for (; it < iters; ++it) {
+                const int s = it % kWgStages;
+                if (it >= kWgStages && !wait_bar(empty0 + 8 * s, ((it / kWgStages) - 1) & 1, abort)) {
+                    ok = false;
+                    break;
+                }
+                long k = k0 + it;
+                const int x0 = int(k % bx) * kWgBoxX;
+                k /= bx;
+                const int y0 = int(k % by) * kWgBoxY, b = int(k / by);
+                const uint32_t st = smem_u32(smem + s * stage_bytes), bar = full0 + 8 * s;
+                bar_expect_tx(bar, stage_bytes);
+                tma_load_4d(st, &tm_dy, 0, x0, y0, b, bar);
+                tma_load_4d(st + kWgBox, &tm_dy, 64, x0, y0, b, bar);
+                for (int j = 0; j < nb; ++j) tma_load_4d(st + (2 + j) * kWgBox, &tm_x, 64 * j, x0 + dx, y0 + dy, b, bar);
+            }
+            for (int k = it > kWgStages ? it - kWgStages : 0; k < it; ++k)
+                if (!wait_bar(full0 + 8 * (k % kWgStages), (k / kWgStages) & 1, nullptr)) ok = false;
+        }
+    } else if (warp == 1) {
+        if (lane == 0) {
+            // kind::f16: f32 accumulate, A and B bf16, both MN-major (bits 15,
+            // 16), N >> 3 at bit 17, M = 128 >> 4 at bit 24.
+            const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | (1u << 15) | (1u << 16) |
+                                   (uint32_t(N >> 3) << 17) | (uint32_t(128 >> 4) << 24);
+            for (int it = 0; it < iters; ++it) {
+                const int s = it % kWgStages;
+                if (!wait_bar(full0 + 8 * s, (it / kWgStages) & 1, abort)) {
+                    ok = false;
+                    break;
+                }
+                fence_after();
+                const uint32_t st = smem_u32(smem + s * stage_bytes);
+                const uint64_t ad = mn_sw128_desc(st), bd = mn_sw128_desc(st + 2 * kWgBox);
+#pragma unroll
+                for (int k = 0; k < kWgK / 16; ++k)  // K = 16 rows = two 1024-byte groups per MMA
+                    mma_bf16(tmem, ad + uint64_t(k * (2048 >> 4)), bd + uint64_t(k * (2048 >> 4)), idesc,
+                             (it | k) != 0);
+                mma_commit(empty0 + 8 * s);
+            }
+            mma_commit(done);
+        }
+    } else {
+        const int q = warp & 3;
+        const int co = q * 32 + lane;
+        if (iters > 0 && __all_sync(0xffffffffu, wait_bar(done, 0, abort))) {
+            fence_after();
+            for (int c = 0; c < N; c += 16) {
+                float v[16];
+                tmem_ld16(tmem + (uint32_t(q * 32) << 16) + uint32_t(c), v);
+                if (co >= Cout) continue;
+                float* dst = dw + (size_t(co) * 9 + tap) * Cin + c;
+#pragma unroll
+                for (int j = 0; j < 16; ++j)
+                    if (c + j < Cin) atomicAdd(dst + j, v[j]);
+            }
+        } else if (iters > 0) {
+            ok = false;
+        }
+    }
+
+    if (!ok) {
+        *abort = 1;
+        atomicOr(status, 1u);
+    }
+    fence_before();
+    __syncthreads();
+    if (warp == 1) {
+        fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(tmem_cols) : "memory");
+    }
+}
 
 }  // namespace
 
@@ -325,22 +532,67 @@ cudaError_t conv_fwd_tc(const ConvShape& s, const __nv_bfloat16* in, const __nv_
             return cudaErrorNotSupported;
     }
     int cols = 32;
-    while (cols < N) cols *= 2;
+    while (cols < 2 * N) cols *= 2;  // two accumulators
     const size_t smem = smem_bytes(N);
     const long tiles = long((s.W + kTileX - 1) / kTileX) * ((s.H + kTileY - 1) / kTileY) * s.B;
     if (tiles > 0x7fffffffL) return cudaErrorNotSupported;
-    cudaError_t e;
-    if (out_f32) {
-        e = cudaFuncSetAttribute(conv_tc_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
-        if (e) return e;
-        conv_tc_kernel<true><<<unsigned(tiles), kThreads, smem, st>>>(tm_in, tm_w, s.H, s.W, s.Cin, N, cols, bias, relu,
-                                                                      out, out_stride, out_offset, status);
-    } else {
-        e = cudaFuncSetAttribute(conv_tc_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
-        if (e) return e;
-        conv_tc_kernel<false><<<unsigned(tiles), kThreads, smem, st>>>(tm_in, tm_w, s.H, s.W, s.Cin, N, cols, bias,
-                                                                       relu, out, out_stride, out_offset, status);
+    const void* fn = out_f32 ? reinterpret_cast<const void*>(conv_tc_kernel<true>)
+                             : reinterpret_cast<const void*>(conv_tc_kernel<false>);
+    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    if (e) return e;
+    const long g = grid_size(N, cols, smem, fn);
+    const unsigned blocks = unsigned(tiles < g ? tiles : g);
+    if (out_f32)
+        conv_tc_kernel<true><<<blocks, kThreads, smem, st>>>(tm_in, tm_w, s.B, s.H, s.W, s.Cin, N, cols, bias, relu,
+                                                             out, out_stride, out_offset, status);
+    else
+        conv_tc_kernel<false><<<blocks, kThreads, smem, st>>>(tm_in, tm_w, s.B, s.H, s.W, s.Cin, N, cols, bias, relu,
+                                                              out, out_stride, out_offset, status);
+    return cudaGetLastError();
+}
+
+cudaError_t conv_wgrad_tc(const ConvShape& s, const __nv_bfloat16* in, const __nv_bfloat16* dout, float* dw,
+                          unsigned int* status, cudaStream_t st) {
+    const int N = (s.Cin + 63) / 64 * 64;
+    if (s.Cout > 128 || s.Cout % 8 || s.Cin % 8 || N > 256 || s.B < 1 || s.H < 1 || s.W < 1)
+        return cudaErrorNotSupported;
+    if ((reinterpret_cast<uintptr_t>(in) | reinterpret_cast<uintptr_t>(dout)) % 16) return cudaErrorNotSupported;
+    PFN_cuTensorMapEncodeTiled_v12000 encode = encode_fn();
+    if (!encode) return cudaErrorNotSupported;
+    CUtensorMap tm_dy, tm_x;
+    const cuuint32_t box[4] = {64, kWgBoxX, kWgBoxY, 1};
+    const cuuint32_t estr[4] = {1, 1, 1, 1};
+    {
+        const cuuint64_t dims[4] = {cuuint64_t(s.Cout), cuuint64_t(s.W), cuuint64_t(s.H), cuuint64_t(s.B)};
+        const cuuint64_t strides[3] = {cuuint64_t(s.Cout) * 2, cuuint64_t(s.W) * s.Cout * 2,
+                                       cuuint64_t(s.H) * s.W * s.Cout * 2};
+        if (encode(&tm_dy, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<__nv_bfloat16*>(dout), dims, strides, box,
+                   estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+            return cudaErrorNotSupported;
     }
+    {
+        const cuuint64_t dims[4] = {cuuint64_t(s.Cin), cuuint64_t(s.W), cuuint64_t(s.H), cuuint64_t(s.B)};
+        const cuuint64_t strides[3] = {cuuint64_t(s.Cin) * 2, cuuint64_t(s.W) * s.Cin * 2,
+                                       cuuint64_t(s.H) * s.W * s.Cin * 2};
+        if (encode(&tm_x, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<__nv_bfloat16*>(in), dims, strides, box,
+                   estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+            return cudaErrorNotSupported;
+    }
+    int cols = 32;
+    while (cols < N) cols *= 2;
+    const size_t smem = 1024 + kWgStages * size_t(2 + N / 64) * kWgBox + (2 * kWgStages + 1) * 8 + 8;
+    cudaError_t e = cudaFuncSetAttribute(wgrad_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    if (e) return e;
+    const long boxes = long((s.W + kWgBoxX - 1) / kWgBoxX) * ((s.H + kWgBoxY - 1) / kWgBoxY) * s.B;
+    // About two CTAs per SM over the 9 taps, at least 8 boxes each.
+    const int target = grid_size(N, cols, smem, reinterpret_cast<const void*>(wgrad_tc_kernel));
+    long splits = (2L * target + 8) / 9;
+    if (splits > boxes / 8) splits = boxes / 8;
+    if (splits < 1) splits = 1;
+    wgrad_tc_kernel<<<unsigned(9 * splits), kThreads, smem, st>>>(tm_dy, tm_x, s.B, s.H, s.W, s.Cin, s.Cout, N, cols,
+                                                                 int(splits), dw, status);
     return cudaGetLastError();
 }
 

@@ -1,0 +1,228 @@
+"""Training and use of the learned denoiser on frames this tracer renders.
+
+* Training set: procedural scenes from fresh seeds of the random-spheres,
+  room-mesh and instancing generators, each seen through a jittered camera,
+  rendered at low spp (inputs, several spp levels so the network meets every
+  noise level it is used at) and at high spp with other sample numbers
+  (targets). Inputs carry the renderer's albedo and normal guides and the
+  primary-ray depth.
+* Training: random crops, Adam on the mean L1 distance of log radiance
+  (pt_unet_train_step, the library's own forward and backward kernels).
+* Use: render + depth guide + pt_denoise_unet, all on the device.
+
+Command line (writes the weights as bfloat16 bits, the precision the network
+computes in):
+    python -m photon_tracer_b200.denoiser train --out weights.npy
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import time
+from typing import Dict, List
+
+import numpy as np
+
+from . import abi
+from .api import Generated, Scene, camera_look_at
+from .unet import UNet, conv_flops, primary_depth
+
+WEIGHTS = os.path.join(os.path.dirname(os.path.abspath(__file__)), "weights", "unet_bf16.npy")
+
+# kind -> (generator, lookfrom, lookat, vfov, camera jitter scale)
+SCENES = {
+    "spheres": (abi.PT_GEN_RANDOM_SPHERES, (13.0, 2.0, 3.0), (0.0, 0.0, 0.0), 20.0, 1.5),
+    "room": (abi.PT_GEN_ROOM_MESH, (0.0, 0.0, 3.3), (0.0, 0.0, 0.0), 40.0, 0.25),
+    "instances": (abi.PT_GEN_INSTANCES, (0.0, 35.0, 140.0), (0.0, 0.0, 0.0), 45.0, 12.0),
+}
+INPUT_SPP = (1, 2, 4, 8, 16, 32)
+TARGET_FIRST_SAMPLE = 1 << 22  # target samples are numbered apart from the inputs'
+
+
+def _stream() -> int:
+    import torch
+    return torch.cuda.current_stream().cuda_stream
+
+
+def render(scene: Scene, cam, width: int, height: int, spp: int, seed: int, first_sample: int = 0,
+           aux: bool = True, max_bounces: int = 10):
+    """(colour [H, W, 3], guides [H, W, 7] or None) on the device."""
+    import torch
+    out = torch.empty((height, width, 3), dtype=torch.float32, device="cuda")
+    ax = torch.empty((height, width, 7), dtype=torch.float32, device="cuda") if aux else None
+    st = Scene.settings(width, height, spp, max_bounces, seed, first_sample, abi.PT_MODE_MEGAKERNEL,
+                        abi.PT_RNG_SAMPLE)
+    scene.render_device(cam, st, out.data_ptr(), ax.data_ptr() if aux else 0, 0, _stream())
+    return out, ax
+
+
+def network_input(color, aux, depth):
+    import torch
+    return torch.cat([color, aux[..., 0:6], depth[..., None]], dim=-1)
+
+
+def scene_and_camera(kind: str, seed: int, aspect: float, jitter: bool):
+    gen, frm, at, vfov, scale = SCENES[kind]
+    g = Generated(gen, seed=seed)
+    frm, at = np.array(frm), np.array(at)
+    if jitter:
+        rng = np.random.default_rng(seed * 7919 + 17)
+        frm = frm + rng.normal(0, scale, 3) * np.array([1.0, 0.4, 1.0])
+        at = at + rng.normal(0, scale * 0.15, 3)
+        vfov = vfov * float(rng.uniform(0.75, 1.25))
+    cam = camera_look_at(tuple(frm), tuple(at), vfov, aspect)
+    return g, Scene(g), cam
+
+
+def make_training_set(frames_per_kind: int, size: int, target_spp: int, seed0: int = 100,
+                      kinds=("spheres", "room", "instances"), log=print) -> List[Dict]:
+    """Per frame: 'inputs' [len(INPUT_SPP), size, size, 10] and 'target' [size, size, 3] on the device."""
+    import torch
+    data = []
+    for k, kind in enumerate(kinds):
+        for f in range(frames_per_kind):
+            seed = seed0 + 1000 * k + f
+            t0 = time.perf_counter()
+            g, scene, cam = scene_and_camera(kind, seed, 1.0, jitter=True)
+            depth = primary_depth(scene, cam, size, size)
+            inputs = []
+            for i, spp in enumerate(INPUT_SPP):
+                c, a = render(scene, cam, size, size, spp, seed, first_sample=0)
+                inputs.append(network_input(c, a, depth))
+            target, _ = render(scene, cam, size, size, target_spp, seed, first_sample=TARGET_FIRST_SAMPLE, aux=False)
+            scene.sync(_stream())
+            data.append({"inputs": torch.stack(inputs).contiguous(), "target": target, "kind": kind, "seed": seed})
+            del scene, g
+            log(f"frame {kind} seed {seed}: {time.perf_counter() - t0:.2f} s")
+    return data
+
+
+def sample_batch(data, rng, batch: int, crop: int):
+    import torch
+    xs, ts = [], []
+    for _ in range(batch):
+        d = data[int(rng.integers(len(data)))]
+        L, H, W, _ = d["inputs"].shape
+        lvl = int(rng.integers(L))
+        y, x = int(rng.integers(H - crop + 1)), int(rng.integers(W - crop + 1))
+        xs.append(d["inputs"][lvl, y:y + crop, x:x + crop])
+        ts.append(d["target"][y:y + crop, x:x + crop])
+    return torch.stack(xs).contiguous(), torch.stack(ts).contiguous()
+
+
+def train(net: UNet, data, steps: int, batch: int = 8, crop: int = 128, lr: float = 1e-3, seed: int = 0,
+          max_seconds: float = float("inf"), log=print) -> List[float]:
+    """Adam at lr for the first 80% of the steps, then lr/10; stops early
+    after max_seconds (the step count then shrinks to what ran)."""
+    rng = np.random.default_rng(seed)
+    losses = []
+    t0 = time.perf_counter()
+    for s in range(steps):
+        if time.perf_counter() - t0 > max_seconds:
+            log(f"stopped after {s} steps (time limit)")
+            break
+        x, t = sample_batch(data, rng, batch, crop)
+        losses.append(net.train_step(x, t, lr if s < 0.8 * steps else lr * 0.1))
+        if (s + 1) % max(1, steps // 20) == 0:
+            log(f"step {s + 1}/{steps}: loss {np.mean(losses[-50:]):.4f} ({time.perf_counter() - t0:.1f} s)")
+    return losses
+
+
+def save_bf16(params: np.ndarray, path: str) -> None:
+    """float32 -> bfloat16 bits (round to nearest even), as uint16."""
+    u = np.ascontiguousarray(params, np.float32).view(np.uint32)
+    r = ((u + 0x7FFF + ((u >> 16) & 1)) >> 16).astype(np.uint16)
+    os.makedirs(os.path.dirname(os.path.abspath(path)), exist_ok=True)
+    np.save(path, r)
+
+
+def load_bf16(path: str) -> np.ndarray:
+    return (np.load(path).astype(np.uint32) << 16).view(np.float32)
+
+
+def trained(path: str = WEIGHTS) -> UNet:
+    """A network with the committed trained weights."""
+    if not os.path.exists(path):
+        raise FileNotFoundError(f"no trained denoiser weights at {path}")
+    net = UNet(seed=0)
+    net.set_params(load_bf16(path))
+    return net
+
+
+def denoise_frame(net: UNet, scene: Scene, cam, width: int, height: int, spp: int, seed: int, max_bounces: int = 10):
+    """Render with guides, depth guide, network -- all enqueued on the current stream."""
+    color, aux = render(scene, cam, width, height, spp, seed, max_bounces=max_bounces)
+    depth = primary_depth(scene, cam, width, height)
+    return color, net.denoise(color, aux, depth)
+
+
+def time_forward(net: UNet, width: int = 1920, height: int = 1080, reps: int = 10) -> Dict:
+    """GPU time of the network at one frame size, tensor cores on and off."""
+    import torch
+    color = torch.rand((height, width, 3), device="cuda")
+    aux = torch.rand((height, width, 7), device="cuda")
+    depth = torch.rand((height, width), device="cuda")
+    out = {}
+    for tc in (True, False):
+        net.tensor_cores(tc)
+        for _ in range(2):
+            net.denoise(color, aux, depth)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        n = reps if tc else max(1, reps // 5)
+        torch.cuda.synchronize()
+        a.record()
+        for _ in range(n):
+            net.denoise(color, aux, depth)
+        b.record()
+        torch.cuda.synchronize()
+        ms = a.elapsed_time(b) / n
+        hp, wp = (height + 7) // 8 * 8, (width + 7) // 8 * 8
+        out["tensor_cores" if tc else "cuda_cores"] = {"ms": round(ms, 3),
+                                                       "tflops": round(conv_flops(1, hp, wp) / ms / 1e9, 1)}
+    net.tensor_cores(True)
+    return out
+
+
+def main(argv=None) -> int:
+    ap = argparse.ArgumentParser(description="train the learned denoiser on frames this tracer renders")
+    sub = ap.add_subparsers(dest="cmd", required=True)
+    t = sub.add_parser("train")
+    t.add_argument("--out", required=True)
+    t.add_argument("--frames", type=int, default=16, help="frames per scene kind")
+    t.add_argument("--size", type=int, default=384)
+    t.add_argument("--target-spp", type=int, default=1024)
+    t.add_argument("--steps", type=int, default=3000)
+    t.add_argument("--batch", type=int, default=8)
+    t.add_argument("--crop", type=int, default=128)
+    t.add_argument("--lr", type=float, default=1e-3)
+    t.add_argument("--init", default=None, help="start from these weights")
+    t.add_argument("--max-minutes", type=float, default=float("inf"), help="stop training after this long")
+    p = sub.add_parser("time")
+    p.add_argument("--width", type=int, default=1920)
+    p.add_argument("--height", type=int, default=1080)
+    args = ap.parse_args(argv)
+    import torch
+    torch.cuda.init()
+    if args.cmd == "time":
+        print(json.dumps(time_forward(UNet(seed=1), args.width, args.height)))
+        return 0
+    t0 = time.perf_counter()
+    data = make_training_set(args.frames, args.size, args.target_spp)
+    t_data = time.perf_counter() - t0
+    net = UNet(seed=1)
+    if args.init:
+        net.set_params(load_bf16(args.init))
+    t0 = time.perf_counter()
+    losses = train(net, data, args.steps, args.batch, args.crop, args.lr, max_seconds=60 * args.max_minutes)
+    t_train = time.perf_counter() - t0
+    save_bf16(net.params(), args.out)
+    np.save(os.path.splitext(args.out)[0] + "_losses.npy", np.array(losses, np.float32))
+    print(json.dumps({"frames": len(data), "data_s": round(t_data, 1), "train_s": round(t_train, 1),
+                      "steps": len(losses), "final_loss": float(np.mean(losses[-100:])),
+                      "ms_per_step": round(1000 * t_train / max(1, len(losses)), 2)}))
+    return 0
+
+
+if __name__ == "__main__":
+    raise SystemExit(main())

@@ -7,7 +7,8 @@
   numbering, pt_accumulate_pass adding each pass's averages * spp in double).
 * time_to_error: the smallest power-of-two spp whose image reaches a relMSE
   target against ground truth, for plain path tracing and for path tracing
-  followed by a denoiser, with the GPU time each took.
+  followed by a denoiser (the a-trous filter or the learned U-Net), with the
+  GPU time each took.
 """
 from __future__ import annotations
 
@@ -121,13 +122,39 @@ def render_and_denoise(scene, cam, width, height, spp, seed, max_bounces=10):
     return out.cpu().numpy(), den.cpu().numpy(), ms
 
 
+def render_and_unet(net, scene, cam, width, height, spp, seed, max_bounces=10):
+    """A frame with its guides and depth, then the learned denoiser, all on the
+    device. Returns (noisy image, denoised image, GPU ms of render + depth + network)."""
+    from .denoiser import denoise_frame
+    res = {}
+
+    def run():
+        res["noisy"], res["den"] = denoise_frame(net, scene, cam, width, height, spp, seed, max_bounces)
+    ms = _timed(run)
+    scene.sync(torch_stream())
+    net.sync()
+    return res["noisy"].cpu().numpy(), res["den"].cpu().numpy(), ms
+
+
+def torch_stream() -> int:
+    import torch
+    return torch.cuda.current_stream().cuda_stream
+
+
 def time_to_error(scene, cam, width: int, height: int, truth: np.ndarray, seed: int = 7, target: float = 0.01,
-                  max_spp: int = 4096, denoise: Optional[str] = None, max_bounces: int = 10) -> dict:
+                  max_spp: int = 4096, denoise: Optional[str] = None, max_bounces: int = 10, net=None) -> dict:
     """The smallest power-of-two spp reaching relMSE <= target, and its GPU time.
-    denoise None: plain path tracing; "atrous": followed by the a-trous filter."""
+    denoise None: plain path tracing; "atrous": followed by the a-trous filter;
+    "unet": followed by the learned denoiser `net`."""
     import torch
     out = torch.empty((height, width, 3), dtype=torch.float32, device="cuda")
     stream = torch.cuda.current_stream().cuda_stream
+    # One untimed pass first: the denoisers allocate their workspaces for a
+    # frame size on first use.
+    if denoise == "unet":
+        render_and_unet(net, scene, cam, width, height, 1, seed + 1, max_bounces)
+    elif denoise is not None:
+        render_and_denoise(scene, cam, width, height, 1, seed + 1, max_bounces)
     history = []
     spp = 1
     while spp <= max_spp:
@@ -136,6 +163,8 @@ def time_to_error(scene, cam, width: int, height: int, truth: np.ndarray, seed: 
             ms = _timed(lambda: scene.render_device(cam, st, out.data_ptr(), 0, 0, stream))
             scene.sync(stream)
             img = out.cpu().numpy()
+        elif denoise == "unet":
+            _, img, ms = render_and_unet(net, scene, cam, width, height, spp, seed, max_bounces)
         else:
             _, img, ms = render_and_denoise(scene, cam, width, height, spp, seed, max_bounces)
         err = relmse(img, truth)

@@ -72,6 +72,10 @@ class UNet:
         assert p.size == self.n_params
         check(self.lib.pt_unet_set_params(self.h, p.ctypes.data_as(C.c_void_p)))
 
+    def sync(self) -> None:
+        """Waits for the current stream; raises if a tensor-core convolution timed out."""
+        check(self.lib.pt_unet_sync(self.h, self._stream()))
+
     def tensor_cores(self, enable: bool) -> None:
         check(self.lib.pt_unet_set_tensor_cores(self.h, int(enable)))
 

@@ -127,54 +127,76 @@ cudaError_t ensure_workspace(pt_unet* n, int B, int H, int W) {
 __nv_bfloat16* w16(pt_unet* n, int l) { return n->params16.as<__nv_bfloat16>() + n->w_off[l]; }
 const float* bias(pt_unet* n, int l) { return n->params.as<float>() + n->b_off[l]; }
 
-cudaError_t conv(pt_unet* n, int l, const void* in, bool in_f32, void* out, bool out_f32, cudaStream_t st) {
+// Convolution l from `in` into `primary` (bf16 or float), with the fused
+// outputs of `o` (concatenation copy or 2x upsample into out2, 2x2 max pool).
+// drop_primary: the tensor-core path need not store `primary` (inference,
+// where only the concatenation reads it). Without tensor cores -- or for a
+// shape they do not take -- conv_fwd writes `primary` and separate kernels
+// produce the fused outputs from it.
+cudaError_t conv(pt_unet* n, int l, const void* in, void* primary, bool out_f32, unet::ConvOut o, bool drop_primary,
+                 cudaStream_t st) {
     const LayerDef& L = kLayers[l];
-    unet::ConvShape s{n->B, n->H >> L.level, n->W >> L.level, L.cin, L.cout};
-    if (n->use_tc && !in_f32) {
+    const int h = n->H >> L.level, w = n->W >> L.level;
+    unet::ConvShape s{n->B, h, w, L.cin, L.cout};
+    o.out = drop_primary ? nullptr : primary;
+    o.stride = L.cout;
+    o.offset = 0;
+    if (n->use_tc) {
         const cudaError_t e = unet::conv_fwd_tc(s, static_cast<const __nv_bfloat16*>(in), w16(n, l), bias(n, l), L.relu,
-                                                out, out_f32, L.cout, 0, n->status.as<unsigned int>(), st);
+                                                o, out_f32, n->status.as<unsigned int>(), st);
         if (e != cudaErrorNotSupported) return e;
     }
-    return unet::conv_fwd(s, in, in_f32, w16(n, l), bias(n, l), L.relu, out, out_f32, L.cout, 0, st);
+    cudaError_t e = unet::conv_fwd(s, in, false, w16(n, l), bias(n, l), L.relu, primary, out_f32, L.cout, 0, st);
+    const __nv_bfloat16* p = static_cast<const __nv_bfloat16*>(primary);
+    if (!e && o.out2)
+        e = o.up2 ? unet::up_fwd(n->B, h, w, L.cout, p, o.out2, o.stride2, o.offset2, st)
+                  : unet::copy_channels(long(n->B) * h * w, L.cout, p, o.out2, o.stride2, o.offset2, st);
+    if (!e && o.pool) e = unet::pool_fwd(n->B, h, w, L.cout, p, o.pool, st);
+    return e;
 }
 
-// The forward pass from act[0] (the padded input) to act[15] (float, 16 channels).
-cudaError_t forward(pt_unet* n, cudaStream_t st) {
+unet::ConvOut to_cat(pt_unet* n, int l, int up) {
+    unet::ConvOut o;
+    o.out2 = n->cat[l].as<__nv_bfloat16>();
+    const int cat_c[3] = {96, 160, 224};
+    o.stride2 = cat_c[l];
+    o.offset2 = up ? 0 : cat_c[l] - kLayers[2 * l + 1].cout;  // the skip half follows the upsampled half
+    o.up2 = up;
+    return o;
+}
+
+// The forward pass from act[0] (the padded input) to act[15] (float, 16
+// channels). The encoder's second convolution at each level also writes
+// its 2x2-pooled output and its copy into the decoder's concatenation; each
+// decoder level's last convolution (and the bottleneck's) writes its
+// upsampled output into the next finer concatenation.
+cudaError_t forward(pt_unet* n, cudaStream_t st, bool training) {
     cudaError_t e;
     auto A = [&](int i) { return n->act[i].p; };
-    const int B = n->B, H = n->H, W = n->W;
+    const bool drop = !training;
 #define TRY(x) \
     if ((e = (x))) return e
-    TRY(conv(n, 0, A(0), false, A(1), false, st));
-    TRY(conv(n, 1, A(1), false, A(2), false, st));
-    TRY(unet::pool_fwd(B, H, W, 32, n->act[2].as<__nv_bfloat16>(), n->pool[0].as<__nv_bfloat16>(), st));
-    TRY(conv(n, 2, n->pool[0].p, false, A(3), false, st));
-    TRY(conv(n, 3, A(3), false, A(4), false, st));
-    TRY(unet::pool_fwd(B, H / 2, W / 2, 64, n->act[4].as<__nv_bfloat16>(), n->pool[1].as<__nv_bfloat16>(), st));
-    TRY(conv(n, 4, n->pool[1].p, false, A(5), false, st));
-    TRY(conv(n, 5, A(5), false, A(6), false, st));
-    TRY(unet::pool_fwd(B, H / 4, W / 4, 96, n->act[6].as<__nv_bfloat16>(), n->pool[2].as<__nv_bfloat16>(), st));
-    TRY(conv(n, 6, n->pool[2].p, false, A(7), false, st));
-    TRY(conv(n, 7, A(7), false, A(8), false, st));
-    // level 2 decoder: [up(a7) 128 | a5 96]
-    TRY(unet::up_fwd(B, H / 8, W / 8, 128, n->act[8].as<__nv_bfloat16>(), n->cat[2].as<__nv_bfloat16>(), 224, 0, st));
-    TRY(unet::copy_channels(pixels_at(n, 2), 96, n->act[6].as<__nv_bfloat16>(), n->cat[2].as<__nv_bfloat16>(), 224, 128,
-                            st));
-    TRY(conv(n, 8, n->cat[2].p, false, A(9), false, st));
-    TRY(conv(n, 9, A(9), false, A(10), false, st));
-    // level 1 decoder: [up(a9) 96 | a3 64]
-    TRY(unet::up_fwd(B, H / 4, W / 4, 96, n->act[10].as<__nv_bfloat16>(), n->cat[1].as<__nv_bfloat16>(), 160, 0, st));
-    TRY(unet::copy_channels(pixels_at(n, 1), 64, n->act[4].as<__nv_bfloat16>(), n->cat[1].as<__nv_bfloat16>(), 160, 96,
-                            st));
-    TRY(conv(n, 10, n->cat[1].p, false, A(11), false, st));
-    TRY(conv(n, 11, A(11), false, A(12), false, st));
-    // level 0 decoder: [up(a11) 64 | a1 32]
-    TRY(unet::up_fwd(B, H / 2, W / 2, 64, n->act[12].as<__nv_bfloat16>(), n->cat[0].as<__nv_bfloat16>(), 96, 0, st));
-    TRY(unet::copy_channels(pixels_at(n, 0), 32, n->act[2].as<__nv_bfloat16>(), n->cat[0].as<__nv_bfloat16>(), 96, 64,
-                            st));
-    TRY(conv(n, 12, n->cat[0].p, false, A(13), false, st));
-    TRY(conv(n, 13, A(13), false, A(14), false, st));
-    TRY(conv(n, 14, A(14), false, A(15), true, st));
+    TRY(conv(n, 0, A(0), A(1), false, {}, false, st));
+    unet::ConvOut o = to_cat(n, 0, 0);
+    o.pool = n->pool[0].as<__nv_bfloat16>();
+    TRY(conv(n, 1, A(1), A(2), false, o, false, st));
+    TRY(conv(n, 2, n->pool[0].p, A(3), false, {}, false, st));
+    o = to_cat(n, 1, 0);
+    o.pool = n->pool[1].as<__nv_bfloat16>();
+    TRY(conv(n, 3, A(3), A(4), false, o, false, st));
+    TRY(conv(n, 4, n->pool[1].p, A(5), false, {}, false, st));
+    o = to_cat(n, 2, 0);
+    o.pool = n->pool[2].as<__nv_bfloat16>();
+    TRY(conv(n, 5, A(5), A(6), false, o, false, st));
+    TRY(conv(n, 6, n->pool[2].p, A(7), false, {}, false, st));
+    TRY(conv(n, 7, A(7), A(8), false, to_cat(n, 2, 1), drop, st));  // level 2: [up(a7) 128 | a5 96]
+    TRY(conv(n, 8, n->cat[2].p, A(9), false, {}, false, st));
+    TRY(conv(n, 9, A(9), A(10), false, to_cat(n, 1, 1), drop, st));  // level 1: [up(a9) 96 | a3 64]
+    TRY(conv(n, 10, n->cat[1].p, A(11), false, {}, false, st));
+    TRY(conv(n, 11, A(11), A(12), false, to_cat(n, 0, 1), drop, st));  // level 0: [up(a11) 64 | a1 32]
+    TRY(conv(n, 12, n->cat[0].p, A(13), false, {}, false, st));
+    TRY(conv(n, 13, A(13), A(14), false, {}, false, st));
+    TRY(conv(n, 14, A(14), A(15), true, {}, false, st));
     return cudaSuccess;
 }
 
@@ -213,7 +235,10 @@ cudaError_t backward(pt_unet* n, cudaStream_t st) {
         const unet::ConvShape t{B, H >> L.level, W >> L.level, L.cout, L.cin};
         const __nv_bfloat16* wt = n->wt16.as<__nv_bfloat16>() + n->w_off[l];
         if (gout16 && g16) {
-            r = unet::conv_fwd_tc(t, g16, wt, nullptr, false, gin, true, L.cin, 0, n->status.as<unsigned int>(), st);
+            unet::ConvOut o;
+            o.out = gin;
+            o.stride = L.cin;
+            r = unet::conv_fwd_tc(t, g16, wt, nullptr, false, o, true, n->status.as<unsigned int>(), st);
             if (r != cudaErrorNotSupported) return r;
         }
         return unet::conv_fwd(t, gout, true, wt, nullptr, false, gin, true, L.cin, 0, st);
@@ -384,7 +409,7 @@ pt_status pt_unet_forward(pt_unet* n, int B, int H, int W, const float* d_input,
     cudaError_t e = ensure_workspace(n, B, H, W);
     const long px = long(B) * H * W;
     if (!e) e = unet::make_input(px, d_input, n->act[0].as<__nv_bfloat16>(), 32, st);
-    if (!e) e = forward(n, st);
+    if (!e) e = forward(n, st, false);
     if (!e) e = unet::make_output(px, kOutStride, n->act[15].as<float>(), d_output, st);
     return e ? cuda_fail(e, "pt_unet_forward") : PT_OK;
 }
@@ -396,7 +421,7 @@ static pt_status loss_and_grads(pt_unet* n, int B, int H, int W, const float* d_
     cudaError_t e = ensure_workspace(n, B, H, W);
     const long px = long(B) * H * W;
     if (!e) e = unet::make_input(px, d_input, n->act[0].as<__nv_bfloat16>(), 32, st);
-    if (!e) e = forward(n, st);
+    if (!e) e = forward(n, st, true);
     if (!e) e = cudaMemsetAsync(n->loss.p, 0, 4, st);
     if (!e) e = unet::l1_loss(px, kOutStride, n->act[15].as<float>(), d_target, n->gact[15].as<float>(),
                               n->loss.as<float>(), st);
@@ -449,7 +474,7 @@ pt_status pt_denoise_unet(pt_unet* n, int width, int height, const float* d_colo
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     cudaError_t e = ensure_workspace(n, 1, Hp, Wp);
     if (!e) e = unet::frame_input(width, height, Wp, Hp, d_color, d_aux, d_depth, n->act[0].as<__nv_bfloat16>(), 32, st);
-    if (!e) e = forward(n, st);
+    if (!e) e = forward(n, st, false);
     if (!e) e = unet::frame_output(width, height, Wp, kOutStride, n->act[15].as<float>(), d_out, st);
     return e ? cuda_fail(e, "pt_denoise_unet") : PT_OK;
 }

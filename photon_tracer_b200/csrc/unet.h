@@ -42,12 +42,24 @@ cudaError_t adam(long n, float* w, const float* g, float* m, float* v, __nv_bflo
                  cudaStream_t st);
 cudaError_t f32_to_bf16(long n, const float* a, __nv_bfloat16* b, cudaStream_t st);
 
+// Where the tensor-core convolution writes its result (any pointer may be
+// null): out[p * stride + offset + co] (bf16, or float for out_f32); a bf16
+// copy into out2 at the same pixel, or (up2) at the four pixels of the 2x
+// finer level it covers -- the halves of a decoder's concatenation; and the
+// 2x2 max pool of the result into pool ([pixel][Cout], bf16).
+struct ConvOut {
+    void* out = nullptr;
+    int stride = 0, offset = 0;
+    __nv_bfloat16* out2 = nullptr;
+    int stride2 = 0, offset2 = 0, up2 = 0;
+    __nv_bfloat16* pool = nullptr;
+};
+
 // Tensor-core forward convolution (tcgen05, accumulators in TMEM). Returns
 // cudaErrorNotSupported for shapes it does not take (Cin % 32, Cout % 16 or
-// Cout > 256), which then run on conv_fwd.
+// Cout > 256; odd sizes with pool), which then run on conv_fwd.
 cudaError_t conv_fwd_tc(const ConvShape& s, const __nv_bfloat16* in, const __nv_bfloat16* w, const float* bias,
-                        bool relu, void* out, bool out_f32, int out_stride, int out_offset, unsigned int* status,
-                        cudaStream_t st);
+                        bool relu, const ConvOut& o, bool out_f32, unsigned int* status, cudaStream_t st);
 
 // Tensor-core weight gradient (tcgen05, MN-major operands): dw += d loss /
 // d w from the layer input and the bf16 gradient of its output (Cout <= 128,

@@ -10,6 +10,8 @@
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
+#include <cstdint>
+
 #include "unet.h"
 
 namespace {
@@ -265,17 +267,34 @@ __global__ void add_channels_kernel(long pixels, int C, const float* __restrict_
         dst[i] += src[(i / C) * stride + offset + i % C];
 }
 
+// Stores the 10 guide values of a pixel, zero-padded to `stride` channels
+// (a multiple of 8), as bf16 with 16-byte stores.
+__device__ __forceinline__ void store_input(const float (&g)[10], __nv_bfloat16* __restrict__ d, int stride) {
+    uint32_t w[16];
+#pragma unroll
+    for (int k = 0; k < 16; ++k) {
+        const float a = 2 * k < 10 ? g[2 * k] : 0.0f, b = 2 * k + 1 < 10 ? g[2 * k + 1] : 0.0f;
+        const __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
+        w[k] = *reinterpret_cast<const uint32_t*>(&h);
+    }
+    uint4* q = reinterpret_cast<uint4*>(d);
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+        if (8 * k < stride) q[k] = make_uint4(w[4 * k], w[4 * k + 1], w[4 * k + 2], w[4 * k + 3]);
+    for (int c = 32; c < stride; c += 8) q[c / 8] = make_uint4(0, 0, 0, 0);
+}
+
 // The network input from float channels (radiance 3, albedo 3, normal 3,
 // depth 1 per pixel): log(1 + radiance), albedo, normal, log(1 + depth),
 // zero-padded to `stride` channels, bf16.
 __global__ void input_kernel(long pixels, const float* __restrict__ src, __nv_bfloat16* __restrict__ dst, int stride) {
     for (long p = blockIdx.x * long(blockDim.x) + threadIdx.x; p < pixels; p += long(gridDim.x) * blockDim.x) {
         const float* s = src + p * 10;
-        __nv_bfloat16* d = dst + p * stride;
-        for (int c = 0; c < 3; ++c) d[c] = __float2bfloat16_rn(log1pf(fmaxf(s[c], 0.0f)));
-        for (int c = 3; c < 9; ++c) d[c] = __float2bfloat16_rn(s[c]);
-        d[9] = __float2bfloat16_rn(log1pf(fmaxf(s[9], 0.0f)));
-        for (int c = 10; c < stride; ++c) d[c] = __float2bfloat16_rn(0.0f);
+        float g[10];
+        for (int c = 0; c < 3; ++c) g[c] = log1pf(fmaxf(s[c], 0.0f));
+        for (int c = 3; c < 9; ++c) g[c] = s[c];
+        g[9] = log1pf(fmaxf(s[9], 0.0f));
+        store_input(g, dst + p * stride, stride);
     }
 }
 
@@ -289,11 +308,11 @@ __global__ void frame_input_kernel(int W, int H, int Wp, int Hp, const float* __
     for (long p = blockIdx.x * long(blockDim.x) + threadIdx.x; p < n; p += long(gridDim.x) * blockDim.x) {
         const int x = min(int(p % Wp), W - 1), y = min(int(p / Wp), H - 1);
         const size_t q = size_t(y) * W + x;
-        __nv_bfloat16* d = dst + p * stride;
-        for (int c = 0; c < 3; ++c) d[c] = __float2bfloat16_rn(log1pf(fmaxf(color[3 * q + c], 0.0f)));
-        for (int c = 0; c < 6; ++c) d[3 + c] = __float2bfloat16_rn(aux7[7 * q + c]);
-        d[9] = __float2bfloat16_rn(log1pf(fmaxf(depth[q], 0.0f)));
-        for (int c = 10; c < stride; ++c) d[c] = __float2bfloat16_rn(0.0f);
+        float g[10];
+        for (int c = 0; c < 3; ++c) g[c] = log1pf(fmaxf(color[3 * q + c], 0.0f));
+        for (int c = 0; c < 6; ++c) g[3 + c] = aux7[7 * q + c];
+        g[9] = log1pf(fmaxf(depth[q], 0.0f));
+        store_input(g, dst + p * stride, stride);
     }
 }
 

@@ -20,6 +20,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <algorithm>
 #include <mutex>
 
 #include "unet.h"
@@ -137,6 +138,17 @@ __device__ __forceinline__ void bar_arrive(uint32_t bar) {
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
 }
 
+__device__ __forceinline__ void pack_bf16(const float (&v)[16], uint4& a, uint4& b) {
+    uint32_t w[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+        const __nv_bfloat162 h = __floats2bfloat162_rn(v[2 * j], v[2 * j + 1]);
+        w[j] = *reinterpret_cast<const uint32_t*>(&h);
+    }
+    a = make_uint4(w[0], w[1], w[2], w[3]);
+    b = make_uint4(w[4], w[5], w[6], w[7]);
+}
+
 struct TileGrid {
     int tiles_x, tiles_y, n;
     __device__ void origin(int t, int& x0, int& y0, int& b) const {
@@ -156,8 +168,7 @@ __global__ void __launch_bounds__(kThreads) conv_tc_kernel(const __grid_constant
                                                            const __grid_constant__ CUtensorMap tm_w, int B, int H,
                                                            int W, int Cin, int N, int tmem_cols,
                                                            const float* __restrict__ bias, int relu,
-                                                           void* __restrict__ out, int out_stride, int out_offset,
-                                                           unsigned int* __restrict__ status) {
+                                                           const unet::ConvOut o, unsigned int* __restrict__ status) {
     extern __shared__ uint8_t smem_raw[];
     uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     const uint32_t b_bytes = uint32_t(N) * kKc * 2;
@@ -274,30 +285,66 @@ __global__ void __launch_bounds__(kThreads) conv_tc_kernel(const __grid_constant
             const int px = x0 + (m % kTileX), py = y0 + (m / kTileX);
             const bool valid = px < W && py < H;
             const size_t pix = (size_t(b) * H + (valid ? py : 0)) * W + (valid ? px : 0);
+            // Pooling windows: lanes 0-15 hold tile row 2q, lanes 16-31 row
+            // 2q + 1 (x0, y0 even), so a window is lanes {l, l^1, l^16, l^17}
+            // and its even-x lane of the upper row writes it.
+            const bool pool_writer = valid && !(lane & 17);
+            const size_t ppix = (size_t(b) * (H >> 1) + (py >> 1)) * (W >> 1) + (px >> 1);
             for (int c = 0; c < N; c += 16) {
                 float v[16];
                 tmem_ld16(tmem + (uint32_t(q * 32) << 16) + uint32_t(a * (tmem_cols / 2) + c), v);
-                if (!valid) continue;
 #pragma unroll
                 for (int j = 0; j < 16; ++j) {
                     v[j] += bias ? bias[c + j] : 0.0f;
                     if (relu) v[j] = fmaxf(v[j], 0.0f);
                 }
                 if (OUT_F32) {
-                    float4* dst = reinterpret_cast<float4*>(static_cast<float*>(out) + pix * out_stride + out_offset + c);
+                    if (!valid || !o.out) continue;
+                    float4* dst = reinterpret_cast<float4*>(static_cast<float*>(o.out) + pix * o.stride + o.offset + c);
 #pragma unroll
                     for (int j = 0; j < 4; ++j) dst[j] = make_float4(v[4 * j], v[4 * j + 1], v[4 * j + 2], v[4 * j + 3]);
-                } else {
-                    uint32_t w[8];
+                    continue;
+                }
+                uint4 w0, w1;
+                pack_bf16(v, w0, w1);
+                if (valid && o.out) {
+                    uint4* dst = reinterpret_cast<uint4*>(static_cast<__nv_bfloat16*>(o.out) + pix * o.stride + o.offset + c);
+                    dst[0] = w0;
+                    dst[1] = w1;
+                }
+                if (valid && o.out2) {
+                    if (o.up2) {
+                        // nearest 2x: the four pixels (2px + i, 2py + j) of the finer level
 #pragma unroll
-                    for (int j = 0; j < 8; ++j) {
-                        const __nv_bfloat162 h = __floats2bfloat162_rn(v[2 * j], v[2 * j + 1]);
-                        w[j] = *reinterpret_cast<const uint32_t*>(&h);
+                        for (int j = 0; j < 2; ++j)
+#pragma unroll
+                            for (int i = 0; i < 2; ++i) {
+                                const size_t q2 = (size_t(b) * 2 * H + 2 * py + j) * (2 * W) + 2 * px + i;
+                                uint4* dst = reinterpret_cast<uint4*>(o.out2 + q2 * o.stride2 + o.offset2 + c);
+                                dst[0] = w0;
+                                dst[1] = w1;
+                            }
+                    } else {
+                        uint4* dst = reinterpret_cast<uint4*>(o.out2 + pix * o.stride2 + o.offset2 + c);
+                        dst[0] = w0;
+                        dst[1] = w1;
                     }
-                    uint4* dst =
-                        reinterpret_cast<uint4*>(static_cast<__nv_bfloat16*>(out) + pix * out_stride + out_offset + c);
-                    dst[0] = make_uint4(w[0], w[1], w[2], w[3]);
-                    dst[1] = make_uint4(w[4], w[5], w[6], w[7]);
+                }
+                if (o.pool) {
+                    // max commutes with the monotonic bf16 rounding: pooling the
+                    // floats then rounding equals pooling the stored bf16 values.
+#pragma unroll
+                    for (int j = 0; j < 16; ++j) {
+                        v[j] = fmaxf(v[j], __shfl_xor_sync(0xffffffffu, v[j], 1));
+                        v[j] = fmaxf(v[j], __shfl_xor_sync(0xffffffffu, v[j], 16));
+                    }
+                    if (pool_writer) {
+                        uint4 p0, p1;
+                        pack_bf16(v, p0, p1);
+                        uint4* dst = reinterpret_cast<uint4*>(o.pool + ppix * N + c);
+                        dst[0] = p0;
+                        dst[1] = p1;
+                    }
                 }
             }
             // This warp's reads of the accumulator are done: the MMA warp may reuse it.
@@ -334,22 +381,36 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
 
 size_t smem_bytes(int N) { return 1024 + kStages * (kABytes + size_t(N) * kKc * 2) + (2 * kStages + 4) * 8 + 8; }
 
-// Resident CTAs per SM for this N (shared memory and TMEM columns), and SMs.
-int grid_size(int N, int cols, size_t smem, const void* fn) {
-    static int sms[64] = {0};
+// CTAs that fit on all SMs at once: per SM the minimum over shared memory
+// (with the per-block reservation), threads, registers (the kernel's count
+// rounded to the allocation unit of 8 per thread) and TMEM columns.
+int grid_size(int cols, size_t smem, const void* fn) {
+    struct Dev {
+        int sms = 0, smem_sm = 0, reserved = 0, threads_sm = 0, regs_sm = 0;
+    };
+    static Dev devs[64];
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev < 0 || dev >= 64) dev = 0;
-    if (!sms[dev]) {
+    Dev& d = devs[dev];
+    if (!d.sms) {
+        cudaDeviceGetAttribute(&d.smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
+        cudaDeviceGetAttribute(&d.reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev);
+        cudaDeviceGetAttribute(&d.threads_sm, cudaDevAttrMaxThreadsPerMultiProcessor, dev);
+        cudaDeviceGetAttribute(&d.regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, dev);
         int n = 0;
         cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
-        sms[dev] = n > 0 ? n : 1;
+        d.sms = n > 0 ? n : 1;
     }
-    int per_sm = 1;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kThreads, smem) != cudaSuccess || per_sm < 1)
-        per_sm = 1;
-    const int by_tmem = 512 / cols;
-    return sms[dev] * (per_sm < by_tmem ? per_sm : by_tmem);
+    cudaFuncAttributes fa{};
+    int regs = 64;
+    if (cudaFuncGetAttributes(&fa, fn) == cudaSuccess && fa.numRegs > 0) regs = (fa.numRegs + 7) / 8 * 8;
+    int per_sm = 32;
+    if (d.smem_sm > 0) per_sm = std::min(per_sm, int(size_t(d.smem_sm) / (smem + size_t(d.reserved))));
+    if (d.threads_sm > 0) per_sm = std::min(per_sm, d.threads_sm / kThreads);
+    if (d.regs_sm > 0) per_sm = std::min(per_sm, d.regs_sm / (regs * kThreads));
+    per_sm = std::min(per_sm, 512 / cols);
+    return d.sms * std::max(per_sm, 1);
 }
 
 // ---- weight gradient -------------------------------------------------------
@@ -498,14 +559,17 @@ __global__ void __launch_bounds__(kThreads) wgrad_tc_kernel(const __grid_constan
 namespace unet {
 
 cudaError_t conv_fwd_tc(const ConvShape& s, const __nv_bfloat16* in, const __nv_bfloat16* w, const float* bias,
-                        bool relu, void* out, bool out_f32, int out_stride, int out_offset, unsigned int* status,
-                        cudaStream_t st) {
+                        bool relu, const ConvOut& o, bool out_f32, unsigned int* status, cudaStream_t st) {
     const int N = s.Cout;
     const int esz = out_f32 ? 4 : 2;
     if (s.Cin % kKc || N % 16 || N < 16 || N > 256 || s.B < 1 || s.H < 1 || s.W < 1) return cudaErrorNotSupported;
     if ((reinterpret_cast<uintptr_t>(in) | reinterpret_cast<uintptr_t>(w)) % 16) return cudaErrorNotSupported;
-    if (reinterpret_cast<uintptr_t>(out) % 16 || (size_t(out_offset) * esz) % 16 || (size_t(out_stride) * esz) % 16)
+    if (reinterpret_cast<uintptr_t>(o.out) % 16 || (size_t(o.offset) * esz) % 16 || (size_t(o.stride) * esz) % 16)
         return cudaErrorNotSupported;
+    if (out_f32 && (o.out2 || o.pool)) return cudaErrorNotSupported;
+    if (reinterpret_cast<uintptr_t>(o.out2) % 16 || (size_t(o.offset2) * 2) % 16 || (size_t(o.stride2) * 2) % 16)
+        return cudaErrorNotSupported;
+    if (o.pool && (reinterpret_cast<uintptr_t>(o.pool) % 16 || s.H % 2 || s.W % 2)) return cudaErrorNotSupported;
     PFN_cuTensorMapEncodeTiled_v12000 encode = encode_fn();
     if (!encode) return cudaErrorNotSupported;
 
@@ -540,14 +604,14 @@ cudaError_t conv_fwd_tc(const ConvShape& s, const __nv_bfloat16* in, const __nv_
                              : reinterpret_cast<const void*>(conv_tc_kernel<false>);
     cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
     if (e) return e;
-    const long g = grid_size(N, cols, smem, fn);
+    const long g = grid_size(cols, smem, fn);
     const unsigned blocks = unsigned(tiles < g ? tiles : g);
     if (out_f32)
-        conv_tc_kernel<true><<<blocks, kThreads, smem, st>>>(tm_in, tm_w, s.B, s.H, s.W, s.Cin, N, cols, bias, relu,
-                                                             out, out_stride, out_offset, status);
+        conv_tc_kernel<true><<<blocks, kThreads, smem, st>>>(tm_in, tm_w, s.B, s.H, s.W, s.Cin, N, cols, bias, relu, o,
+                                                             status);
     else
-        conv_tc_kernel<false><<<blocks, kThreads, smem, st>>>(tm_in, tm_w, s.B, s.H, s.W, s.Cin, N, cols, bias, relu,
-                                                              out, out_stride, out_offset, status);
+        conv_tc_kernel<false><<<blocks, kThreads, smem, st>>>(tm_in, tm_w, s.B, s.H, s.W, s.Cin, N, cols, bias, relu, o,
+                                                              status);
     return cudaGetLastError();
 }
 
@@ -587,7 +651,7 @@ cudaError_t conv_wgrad_tc(const ConvShape& s, const __nv_bfloat16* in, const __n
     if (e) return e;
     const long boxes = long((s.W + kWgBoxX - 1) / kWgBoxX) * ((s.H + kWgBoxY - 1) / kWgBoxY) * s.B;
     // About two CTAs per SM over the 9 taps, at least 8 boxes each.
-    const int target = grid_size(N, cols, smem, reinterpret_cast<const void*>(wgrad_tc_kernel));
+    const int target = grid_size(cols, smem, reinterpret_cast<const void*>(wgrad_tc_kernel));
     long splits = (2L * target + 8) / 9;
     if (splits > boxes / 8) splits = boxes / 8;
     if (splits < 1) splits = 1;

@@ -161,7 +161,7 @@ pt_status launch_render(pt_scene* s, PtRenderParams& p, int mode, cudaStream_t s
     PtLaunchShape shape;
     shape.threads = 128;
     if (!s->blocks_per_sm[variant])
-        s->blocks_per_sm[variant] = pt_megakernel_blocks_per_sm(shape.threads, p.aux != nullptr,
+        s->blocks_per_sm[variant] = pt_megakernel_blocks_per_sm(s->dev, shape.threads, p.aux != nullptr,
                                                                 p.rng_mode == PT_RNG_SNAPSHOT);
     shape.blocks = s->sms * s->blocks_per_sm[variant];
     p.work = s->work;

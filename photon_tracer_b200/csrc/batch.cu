@@ -12,6 +12,7 @@
 // it alone. Each scene's completion time is taken from the global timer
 // when its last pixel is written.
 #include "batch.h"
+#include "kernels.h"
 #include "path.cuh"
 
 using namespace ptd;
@@ -171,9 +172,7 @@ __global__ void __launch_bounds__(THREADS, 384 / THREADS) batch_megakernel(PtSce
 
 template <int THREADS>
 int blocks_per_sm() {
-    int n = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, batch_megakernel<THREADS>, THREADS, 0) != cudaSuccess) n = 1;
-    return n > 0 ? n : 1;
+    return pt_resident_blocks(reinterpret_cast<const void*>(batch_megakernel<THREADS>), THREADS, 0);
 }
 
 }  // namespace

@@ -34,7 +34,7 @@ struct PtLaunchShape {
 // renders its pixel's samples one path after another.
 cudaError_t pt_launch_megakernel(const PtSceneDev& scene, const PtRenderParams& p, const PtLaunchShape& shape,
                                  cudaStream_t stream);
-int pt_megakernel_blocks_per_sm(int threads, bool aux, bool snapshot);
+int pt_megakernel_blocks_per_sm(const PtSceneDev& scene, int threads, bool aux, bool snapshot);
 
 // Ray queries: closest hit (pt_hit records), any hit (bytes), and traversal
 // work counters (5 x u64, added to).
@@ -49,3 +49,8 @@ cudaError_t pt_launch_trace_count(const PtSceneDev& scene, const float* rays, si
 // (0 on a miss).
 cudaError_t pt_launch_primary_depth(const PtSceneDev& scene, const PtCamDev& cam, int width, int height, float* depth,
                                     cudaStream_t stream);
+
+// Blocks of `threads` threads (and dyn_smem bytes of dynamic shared memory)
+// of kernel fn that fit on one SM at once, from the device's limits and the
+// kernel's registers and static shared memory.
+int pt_resident_blocks(const void* fn, int threads, size_t dyn_smem);

@@ -23,6 +23,7 @@
 #include <algorithm>
 #include <mutex>
 
+#include "kernels.h"
 #include "unet.h"
 
 namespace {
@@ -381,36 +382,20 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
 
 size_t smem_bytes(int N) { return 1024 + kStages * (kABytes + size_t(N) * kKc * 2) + (2 * kStages + 4) * 8 + 8; }
 
-// CTAs that fit on all SMs at once: per SM the minimum over shared memory
-// (with the per-block reservation), threads, registers (the kernel's count
-// rounded to the allocation unit of 8 per thread) and TMEM columns.
+// CTAs that fit on all SMs at once: the kernel's resident blocks per SM
+// (shared memory, threads, registers), capped by the TMEM columns each holds.
 int grid_size(int cols, size_t smem, const void* fn) {
-    struct Dev {
-        int sms = 0, smem_sm = 0, reserved = 0, threads_sm = 0, regs_sm = 0;
-    };
-    static Dev devs[64];
+    static int sms[64] = {0};
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev < 0 || dev >= 64) dev = 0;
-    Dev& d = devs[dev];
-    if (!d.sms) {
-        cudaDeviceGetAttribute(&d.smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
-        cudaDeviceGetAttribute(&d.reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev);
-        cudaDeviceGetAttribute(&d.threads_sm, cudaDevAttrMaxThreadsPerMultiProcessor, dev);
-        cudaDeviceGetAttribute(&d.regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, dev);
+    if (!sms[dev]) {
         int n = 0;
         cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
-        d.sms = n > 0 ? n : 1;
+        sms[dev] = n > 0 ? n : 1;
     }
-    cudaFuncAttributes fa{};
-    int regs = 64;
-    if (cudaFuncGetAttributes(&fa, fn) == cudaSuccess && fa.numRegs > 0) regs = (fa.numRegs + 7) / 8 * 8;
-    int per_sm = 32;
-    if (d.smem_sm > 0) per_sm = std::min(per_sm, int(size_t(d.smem_sm) / (smem + size_t(d.reserved))));
-    if (d.threads_sm > 0) per_sm = std::min(per_sm, d.threads_sm / kThreads);
-    if (d.regs_sm > 0) per_sm = std::min(per_sm, d.regs_sm / (regs * kThreads));
-    per_sm = std::min(per_sm, 512 / cols);
-    return d.sms * std::max(per_sm, 1);
+    const int per_sm = std::min(pt_resident_blocks(fn, kThreads, smem), 512 / cols);
+    return sms[dev] * std::max(per_sm, 1);
 }
 
 // ---- weight gradient -------------------------------------------------------

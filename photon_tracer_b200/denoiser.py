@@ -1,10 +1,10 @@
 """Training and use of the learned denoiser on frames this tracer renders.
 
 * Training set: procedural scenes from fresh seeds of the random-spheres,
-  room-mesh and instancing generators, each seen through a jittered camera,
-  rendered at low spp (inputs, several spp levels so the network meets every
-  noise level it is used at) and at high spp with other sample numbers
-  (targets). Inputs carry the renderer's albedo and normal guides and the
+  room-mesh and instancing generators, seen through jittered cameras and
+  through each generator's own camera, rendered at low spp (inputs, several
+  spp levels so the network meets every noise level it is used at) and at
+  high spp with other sample numbers (targets). Inputs carry the renderer's albedo and normal guides and the
   primary-ray depth.
 * Training: random crops, Adam on the mean L1 distance of log radiance
   (pt_unet_train_step, the library's own forward and backward kernels).
@@ -75,26 +75,34 @@ def scene_and_camera(kind: str, seed: int, aspect: float, jitter: bool):
     return g, Scene(g), cam
 
 
-def make_training_set(frames_per_kind: int, size: int, target_spp: int, seed0: int = 100,
-                      kinds=("spheres", "room", "instances"), log=print) -> List[Dict]:
-    """Per frame: 'inputs' [len(INPUT_SPP), size, size, 10] and 'target' [size, size, 3] on the device."""
+def render_pair(kind: str, seed: int, width: int, height: int, target_spp: int, jitter: bool) -> Dict:
+    """One training frame: inputs at every INPUT_SPP level and the target, on the device."""
     import torch
+    g, scene, cam = scene_and_camera(kind, seed, width / height, jitter=jitter)
+    depth = primary_depth(scene, cam, width, height)
+    inputs = []
+    for spp in INPUT_SPP:
+        c, a = render(scene, cam, width, height, spp, seed, first_sample=0)
+        inputs.append(network_input(c, a, depth))
+    target, _ = render(scene, cam, width, height, target_spp, seed, first_sample=TARGET_FIRST_SAMPLE, aux=False)
+    scene.sync(_stream())
+    return {"inputs": torch.stack(inputs).contiguous(), "target": target, "kind": kind, "seed": seed}
+
+
+def make_training_set(frames_per_kind: int, size: int, target_spp: int, seed0: int = 100,
+                      kinds=("spheres", "room", "instances"), default_frames: int = 0, log=print) -> List[Dict]:
+    """Per frame: 'inputs' [len(INPUT_SPP), H, W, 10] and 'target' [H, W, 3] on the device.
+    frames_per_kind square frames of `size` through jittered cameras (seeds
+    seed0 + 1000 k + f), and default_frames 640x360 frames through each
+    generator's own camera (seeds seed0 + 1000 k + 500 + f)."""
     data = []
     for k, kind in enumerate(kinds):
-        for f in range(frames_per_kind):
-            seed = seed0 + 1000 * k + f
+        jobs = [(seed0 + 1000 * k + f, size, size, True) for f in range(frames_per_kind)]
+        jobs += [(seed0 + 1000 * k + 500 + f, 640, 360, False) for f in range(default_frames)]
+        for seed, w, h, jitter in jobs:
             t0 = time.perf_counter()
-            g, scene, cam = scene_and_camera(kind, seed, 1.0, jitter=True)
-            depth = primary_depth(scene, cam, size, size)
-            inputs = []
-            for i, spp in enumerate(INPUT_SPP):
-                c, a = render(scene, cam, size, size, spp, seed, first_sample=0)
-                inputs.append(network_input(c, a, depth))
-            target, _ = render(scene, cam, size, size, target_spp, seed, first_sample=TARGET_FIRST_SAMPLE, aux=False)
-            scene.sync(_stream())
-            data.append({"inputs": torch.stack(inputs).contiguous(), "target": target, "kind": kind, "seed": seed})
-            del scene, g
-            log(f"frame {kind} seed {seed}: {time.perf_counter() - t0:.2f} s")
+            data.append(render_pair(kind, seed, w, h, target_spp, jitter))
+            log(f"frame {kind} seed {seed} {w}x{h}: {time.perf_counter() - t0:.2f} s")
     return data
 
 
@@ -189,7 +197,8 @@ def main(argv=None) -> int:
     sub = ap.add_subparsers(dest="cmd", required=True)
     t = sub.add_parser("train")
     t.add_argument("--out", required=True)
-    t.add_argument("--frames", type=int, default=16, help="frames per scene kind")
+    t.add_argument("--frames", type=int, default=16, help="jittered square frames per scene kind")
+    t.add_argument("--default-frames", type=int, default=0, help="640x360 frames per kind through its own camera")
     t.add_argument("--size", type=int, default=384)
     t.add_argument("--target-spp", type=int, default=1024)
     t.add_argument("--steps", type=int, default=3000)
@@ -208,7 +217,7 @@ def main(argv=None) -> int:
         print(json.dumps(time_forward(UNet(seed=1), args.width, args.height)))
         return 0
     t0 = time.perf_counter()
-    data = make_training_set(args.frames, args.size, args.target_spp)
+    data = make_training_set(args.frames, args.size, args.target_spp, default_frames=args.default_frames)
     t_data = time.perf_counter() - t0
     net = UNet(seed=1)
     if args.init:

@@ -171,6 +171,8 @@ pt_status enqueue_one_launch(pt_batch* b, int threads, cudaStream_t stream) {
     L.done_ns = b->d_done_ns;
     L.start_ns = b->d_start;
     L.rays = b->d_rays;
+    L.any_instances = 0;
+    for (const PtBatchScene& sc : b->scenes) L.any_instances |= sc.inst_root != PT_NONE ? 1 : 0;
     cudaError_t e = cudaMemsetAsync(b->d_work, 0, sizeof(unsigned int), stream);
     if (!e) e = cudaMemsetAsync(b->d_done, 0, b->scenes.size() * sizeof(unsigned int), stream);
     if (!e) e = cudaMemsetAsync(b->d_start, 0xff, sizeof(unsigned long long), stream);

@@ -27,8 +27,15 @@ __device__ __forceinline__ unsigned long long global_ns() {
     return t;
 }
 
-template <int THREADS>
-__global__ void __launch_bounds__(THREADS, 384 / THREADS) batch_megakernel(PtSceneDev S0, PtBatchLaunch B) {
+// Resident 128-thread blocks per SM the register allocation targets (scaled
+// for other block sizes).
+#ifndef PT_BATCH_MIN_BLOCKS128
+#define PT_BATCH_MIN_BLOCKS128 3
+#endif
+
+template <int THREADS, int TREES>
+__global__ void __launch_bounds__(THREADS, PT_BATCH_MIN_BLOCKS128 * 128 / THREADS)
+    batch_megakernel(PtSceneDev S0, PtBatchLaunch B) {
     StackEntry stack[PT_STACK_MAX];
     const int lane = threadIdx.x & 31;
     if (threadIdx.x == 0) atomicMin(B.start_ns, global_ns());
@@ -131,7 +138,7 @@ __global__ void __launch_bounds__(THREADS, 384 / THREADS) batch_megakernel(PtSce
             Hit h;
             Counts cnt;
             Rec rec;
-            if (!closest<false>(S, path.o, path.d, 0.001f, t, h, stack, cnt)) {
+            if (!closest<false, TREES>(S, path.o, path.d, 0.001f, t, h, stack, cnt)) {
                 overflow = true;
                 h.kind = PT_HIT_NONE;
             }
@@ -142,7 +149,7 @@ __global__ void __launch_bounds__(THREADS, 384 / THREADS) batch_megakernel(PtSce
             const int step = shade<false>(S, path, hit, rec, depth, smp, rng, first, nee, sh, rays);
             if (nee) {
                 bool ovf = false;
-                if (!occluded<false>(S, sh.o, sh.d, 0.001f, sh.t_max, stack, cnt, &ovf)) path.rad = path.rad + sh.value;
+                if (!occluded<false, TREES>(S, sh.o, sh.d, 0.001f, sh.t_max, stack, cnt, &ovf)) path.rad = path.rad + sh.value;
                 overflow |= ovf;
             }
             if (step == STEP_DONE) {
@@ -170,24 +177,34 @@ __global__ void __launch_bounds__(THREADS, 384 / THREADS) batch_megakernel(PtSce
     if (__any_sync(0xffffffffu, overflow) && lane == 0) atomicOr(S0.status, PT_DEV_ERR_STACK);
 }
 
-template <int THREADS>
-int blocks_per_sm() {
-    return pt_resident_blocks(reinterpret_cast<const void*>(batch_megakernel<THREADS>), THREADS, 0);
+template <int THREADS, int TREES>
+void launch(const PtSceneDev& S, const PtBatchLaunch& b, int sms, cudaStream_t stream) {
+    const int blocks = pt_resident_blocks(reinterpret_cast<const void*>(batch_megakernel<THREADS, TREES>), THREADS, 0);
+    batch_megakernel<THREADS, TREES><<<sms * blocks, THREADS, 0, stream>>>(S, b);
+}
+
+template <int TREES>
+void launch_threads(const PtSceneDev& S, const PtBatchLaunch& b, int threads, int sms, cudaStream_t stream) {
+    switch (threads) {
+        case 64:
+            launch<64, TREES>(S, b, sms, stream);
+            break;
+        case 256:
+            launch<256, TREES>(S, b, sms, stream);
+            break;
+        default:
+            launch<128, TREES>(S, b, sms, stream);
+            break;
+    }
 }
 
 }  // namespace
 
+// The single-loop traversal when some scene has instances, one loop per tree otherwise.
 cudaError_t pt_launch_batch(const PtSceneDev& S, const PtBatchLaunch& b, int threads, int sms, cudaStream_t stream) {
-    switch (threads) {
-        case 64:
-            batch_megakernel<64><<<sms * blocks_per_sm<64>(), 64, 0, stream>>>(S, b);
-            break;
-        case 256:
-            batch_megakernel<256><<<sms * blocks_per_sm<256>(), 256, 0, stream>>>(S, b);
-            break;
-        default:
-            batch_megakernel<128><<<sms * blocks_per_sm<128>(), 128, 0, stream>>>(S, b);
-            break;
-    }
+    if (b.any_instances)
+        launch_threads<PT_TREES_ONE>(S, b, threads, sms, stream);
+    else
+        launch_threads<PT_TREES_EACH>(S, b, threads, sms, stream);
     return cudaGetLastError();
 }

@@ -30,6 +30,7 @@ struct PtBatchLaunch {
     unsigned long long* done_ns;       // per scene: global timer when its last pixel was written
     unsigned long long* start_ns;      // set to ~0 before the launch; the earliest block start
     unsigned long long* rays;          // added to (may be null)
+    int any_instances;                 // some scene has an instance tree: the single-loop traversal
 };
 
 cudaError_t pt_launch_batch(const PtSceneDev& arena, const PtBatchLaunch& b, int threads, int sms,

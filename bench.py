@@ -360,6 +360,44 @@ def run_unet_workload(args):
     return 0
 
 
+def run_bvh_workload(args):
+    """BVH build on the GPU (pt_bvh_build_gpu) against the host builder
+    (pt_bvh_build, the reference's algorithm): wall time per build of the
+    327,680-triangle room icosphere (subdivision 7) and of 1M random boxes,
+    and whether the trees are identical."""
+    import numpy as np
+    import photon_tracer_b200 as pt
+    from photon_tracer_b200 import abi
+    g = pt.Generated(abi.PT_GEN_ROOM_MESH, seed=SEED, param=7)
+    tris = np.ctypeslib.as_array(g.desc.triangles, (g.desc.n_triangles,))
+    p0, p1, p2 = tris["p0"], tris["p1"], tris["p2"]
+    mesh = np.concatenate([np.minimum(np.minimum(p0, p1), p2) - 1e-4, np.maximum(np.maximum(p0, p1), p2) + 1e-4],
+                          1).astype(np.float32)
+    rng = np.random.default_rng(SEED)
+    c = rng.random((1 << 20, 3)) * 100
+    e = rng.random((1 << 20, 3)) * 0.2
+    rand = np.concatenate([c - e, c + e], 1).astype(np.float32)
+    pt.bvh_build(mesh[:4096], gpu=True)  # load the kernels
+    results = {}
+    for name, boxes in (("room_icosphere_327680_tris", mesh), ("random_1M_boxes", rand)):
+        t = time.perf_counter()
+        nh, oh = pt.bvh_build(boxes)
+        host_s = time.perf_counter() - t
+        times = []
+        for _ in range(max(1, args.steps)):
+            t = time.perf_counter()
+            ng, og = pt.bvh_build(boxes, gpu=True)
+            times.append(time.perf_counter() - t)
+        results[name] = {"host_ms": round(host_s * 1e3, 1), "gpu_ms": round(min(times) * 1e3, 1),
+                         "speedup": round(host_s / min(times), 1), "nodes": int(len(nh)),
+                         "identical": bool(ng.tobytes() == nh.tobytes() and np.array_equal(og, oh))}
+    print(json.dumps({"workload": "bvh", "metric": "BVH build wall time, GPU vs host (same tree)", "unit": "ms",
+                      "higher_is_better": False, "results": results,
+                      "timing": "wall clock around the blocking call, host arrays in and out, best of --steps"}),
+          flush=True)
+    return 0
+
+
 def run_scene_workload(args, kind, label, param=0):
     """Mrays/s of the megakernel on another BASELINE configuration."""
     import torch
@@ -401,7 +439,7 @@ def main():
     ap.add_argument("--mode", default="mega", choices=["mega", "wave"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default="room",
-                    choices=["room", "batch", "convergence", "unet", "instances", "spheres"],
+                    choices=["room", "batch", "convergence", "unet", "bvh", "instances", "spheres"],
                     help="room: the headline line (config 1); the others print their own JSON line")
     ap.add_argument("--seeds", type=int, nargs="+", default=[1001, 1002])
     ap.add_argument("--kinds", nargs="+", default=["spheres", "room", "instances"],
@@ -432,6 +470,8 @@ def main():
             return run_convergence_workload(args)
         if args.workload == "unet":
             return run_unet_workload(args)
+        if args.workload == "bvh":
+            return run_bvh_workload(args)
         if args.workload == "instances":
             return run_scene_workload(args, _abi.PT_GEN_INSTANCES, "instances")
         return run_scene_workload(args, _abi.PT_GEN_RANDOM_SPHERES, "spheres")

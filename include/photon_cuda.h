@@ -212,6 +212,19 @@ typedef struct pt_settings {
     const uint64_t* rng_states; /* PT_RNG_SNAPSHOT only: width*height*spp*4 words */
 } pt_settings;
 
+/* Progressive rendering (the web front end's render loop, web/gpu.js:205-226):
+ * the frame's samples in batches that start at 1 spp and double while a batch
+ * takes under 20 ms (up to 64) or halve above 60 ms, each batch continuing
+ * the per-pixel sample numbering (first_sample + samples done), its averages
+ * summed per pixel in FP64. After each batch but the last, progress (may be
+ * NULL) is called with the samples done so far; a nonzero return stops the
+ * render there. out (host, 3 floats per pixel, top row first) gets the mean
+ * of the samples done, *samples_done (may be NULL) their count. Needs
+ * PT_RNG_SAMPLE; no aux. */
+typedef int (*pt_progress_fn)(void* user, int32_t samples_done, int32_t samples_total);
+pt_status pt_render_progressive(pt_scene* scene, const pt_camera* cam, const pt_settings* settings, float* out,
+                                pt_progress_fn progress, void* user, int32_t* samples_done, uint64_t* rays_out);
+
 /* Renders a frame. Replaces the per-row calls of
  * render_row_linear(world, cam, j, W, H, spp, depth, out, seed, first_sample, aux)
  * (include/renderer.hpp:411-416) over every row, in the layout
@@ -284,6 +297,12 @@ pt_status pt_trace_count(pt_scene* scene, const float* rays, size_t n, float tmi
  * bvh::build (include/bvh.hpp:39-52, 126-247). boxes is n*6 floats (min xyz,
  * max xyz). Free the results with pt_free. */
 pt_status pt_bvh_build(const float* boxes, uint32_t n, pt_bvh_node** nodes, uint32_t* n_nodes, uint32_t** order);
+/* The same build on the GPU (binned SAH over primitive chunks for large
+ * nodes, one thread per subtree of <= 128 primitives, the 4-wide collapse on
+ * the host): the same nodes and order as pt_bvh_build, byte for byte, for
+ * the same boxes (bvh::build, include/bvh.hpp:39-52, 126-247; the reference
+ * builds on the host only). Host arrays in and out; free with pt_free. */
+pt_status pt_bvh_build_gpu(const float* boxes, uint32_t n, pt_bvh_node** nodes, uint32_t* n_nodes, uint32_t** order);
 void pt_free(void* p);
 
 /* ---- denoising -------------------------------------------------------------- */

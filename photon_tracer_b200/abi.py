@@ -140,6 +140,8 @@ ST = C.c_int32
 SIZE = C.c_size_t
 
 # (name, restype, argtypes) of every entry point include/photon_cuda.h declares.
+PROGRESS_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_int32, C.c_int32)
+
 PROTOTYPES = [
     ("pt_last_error", C.c_char_p, []),
     ("pt_version", C.c_char_p, []),
@@ -156,10 +158,14 @@ PROTOTYPES = [
     ("pt_trace_any", ST, [P, P, SIZE, C.c_float, C.c_float, P]),
     ("pt_trace_closest_device", ST, [P, P, SIZE, C.c_float, C.c_float, P, P]),
     ("pt_trace_any_device", ST, [P, P, SIZE, C.c_float, C.c_float, P, P]),
+    ("pt_render_progressive", ST, [P, C.POINTER(pt_camera), C.POINTER(pt_settings), P, PROGRESS_FN, P,
+                                   C.POINTER(C.c_int32), C.POINTER(C.c_uint64)]),
     ("pt_primary_depth_device", ST, [P, C.POINTER(pt_camera), C.c_int, C.c_int, P, P]),
     ("pt_trace_count", ST, [P, P, SIZE, C.c_float, C.c_float, C.POINTER(C.c_uint64)]),
     ("pt_bvh_build", ST, [P, C.c_uint32, C.POINTER(C.POINTER(pt_bvh_node)), C.POINTER(C.c_uint32),
                           C.POINTER(C.POINTER(C.c_uint32))]),
+    ("pt_bvh_build_gpu", ST, [P, C.c_uint32, C.POINTER(C.POINTER(pt_bvh_node)), C.POINTER(C.c_uint32),
+                              C.POINTER(C.POINTER(C.c_uint32))]),
     ("pt_free", None, [P]),
     ("pt_denoise_atrous", ST, [C.c_int, C.c_int, P, P, P, P, P]),
     ("pt_denoise_atrous_device", ST, [C.c_int, C.c_int, P, P, P, P, P, P, P]),

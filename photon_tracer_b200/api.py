@@ -67,15 +67,17 @@ def generate_rays(seed: int, lo, hi, n: int) -> np.ndarray:
 
 
 # ---- BVH --------------------------------------------------------------------------
-def bvh_build(boxes: np.ndarray):
+def bvh_build(boxes: np.ndarray, gpu: bool = False):
     """The library's builder (same nodes and order as the reference's bvh::build).
-    boxes: (n, 6) float32 min xyz, max xyz. Returns (nodes structured array, order)."""
+    boxes: (n, 6) float32 min xyz, max xyz. Returns (nodes structured array, order).
+    gpu: build on the GPU (pt_bvh_build_gpu), the same result."""
     boxes = np.ascontiguousarray(boxes, np.float32)
     lib = load()
     nodes_p = C.POINTER(abi.pt_bvh_node)()
     order_p = C.POINTER(C.c_uint32)()
     nn = C.c_uint32()
-    check(lib.pt_bvh_build(_ptr(boxes), boxes.shape[0], C.byref(nodes_p), C.byref(nn), C.byref(order_p)))
+    fn = lib.pt_bvh_build_gpu if gpu else lib.pt_bvh_build
+    check(fn(_ptr(boxes), boxes.shape[0], C.byref(nodes_p), C.byref(nn), C.byref(order_p)))
     try:
         nodes = np.ctypeslib.as_array(C.cast(nodes_p, C.POINTER(C.c_uint8)), (nn.value * 128,)).copy()
         nodes = nodes.view(abi.NODE_DTYPE) if nn.value else np.zeros(0, abi.NODE_DTYPE)
@@ -162,6 +164,16 @@ class Scene:
         check(load().pt_render_device(self._h, C.byref(cam), C.byref(settings), C.c_void_p(out_ptr),
                                       C.c_void_p(aux_ptr or None), C.c_void_p(rays_ptr or None),
                                       C.c_void_p(stream or None)))
+
+    def render_progressive(self, cam, settings: abi.pt_settings, progress=None):
+        """pt_render_progressive: batches of growing spp summed in FP64.
+        progress(done, total) -> truthy stops early. Returns (image, samples done, rays)."""
+        out = np.empty((settings.height, settings.width, 3), np.float32)
+        done, rays = C.c_int32(), C.c_uint64()
+        cb = abi.PROGRESS_FN(lambda _u, d, t: int(bool(progress(d, t)))) if progress else abi.PROGRESS_FN()
+        check(load().pt_render_progressive(self._h, C.byref(cam), C.byref(settings), _ptr(out), cb, None,
+                                           C.byref(done), C.byref(rays)))
+        return out, done.value, rays.value
 
     def sync(self, stream: int = 0) -> None:
         check(load().pt_sync(self._h, C.c_void_p(stream or None)))

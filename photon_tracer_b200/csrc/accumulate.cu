@@ -19,7 +19,19 @@ __global__ void add_pass(size_t n, const float* __restrict__ frame, double weigh
         sum[i] += double(frame[i]) * weight;
 }
 
+__global__ void mean_of_sum(size_t n, const double* __restrict__ sum, double inv, float* __restrict__ out) {
+    for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x)
+        out[i] = float(sum[i] * inv);
+}
+
 }  // namespace
+
+cudaError_t pt_launch_mean_of_sum(const double* sum, size_t n, double inv, float* out, cudaStream_t stream) {
+    if (n == 0) return cudaSuccess;
+    const size_t blocks = (n + 255) / 256;
+    mean_of_sum<<<unsigned(blocks < 148 * 32 ? blocks : 148 * 32), 256, 0, stream>>>(n, sum, inv, out);
+    return cudaGetLastError();
+}
 
 extern "C" pt_status pt_accumulate_pass(const float* d_frame, size_t n_floats, double weight, double* d_sum,
                                         void* stream) {

@@ -3,6 +3,8 @@
 // pt_status and a message for pt_last_error(). No exception leaves this file.
 #include <cuda_runtime.h>
 
+#include <chrono>
+
 #include <algorithm>
 #include <cstring>
 #include <mutex>
@@ -67,7 +69,7 @@ struct pt_scene {
     unsigned int* work = nullptr;      // megakernel work counter
     unsigned long long* rays = nullptr;
     cudaStream_t stream = nullptr;
-    Scratch out, aux, states, in_rays, out_hits, counts, wave;
+    Scratch out, aux, states, in_rays, out_hits, counts, wave, sum;
     uint32_t* host_counts = nullptr;  // pinned, for the wavefront queue read-back
     int blocks_per_sm[4] = {0, 0, 0, 0};
 };
@@ -293,6 +295,7 @@ pt_status pt_scene_destroy(pt_scene* s) {
     if (s->stream) cudaStreamSynchronize(s->stream);
     s->out.release();
     s->aux.release();
+    s->sum.release();
     s->states.release();
     s->in_rays.release();
     s->out_hits.release();
@@ -365,6 +368,55 @@ pt_status pt_render(pt_scene* s, const pt_camera* cam, const pt_settings* st, fl
     if (cudaError_t e = cudaMemcpyAsync(&rays, s->rays, sizeof(rays), cudaMemcpyDeviceToHost, stream))
         return cuda_fail(e, "pt_render: ray count");
     if (pt_status e = read_status(s, stream)) return e;
+    if (rays_out) *rays_out = rays;
+    return PT_OK;
+}
+
+pt_status pt_render_progressive(pt_scene* s, const pt_camera* cam, const pt_settings* st, float* out,
+                                pt_progress_fn progress, void* user, int32_t* samples_done, uint64_t* rays_out) {
+    clear_error();
+    if (!s || !cam || !out) return fail(PT_ERR_INVALID_ARG, "pt_render_progressive: null pointer");
+    if (pt_status e = check_settings(st)) return e;
+    if (st->rng != PT_RNG_SAMPLE) return fail(PT_ERR_INVALID_ARG, "pt_render_progressive: needs PT_RNG_SAMPLE");
+    if (pt_status e = use_device(s)) return e;
+    const size_t px = size_t(st->width) * st->height;
+    if (pt_status e = s->out.ensure(3 * px * sizeof(float), "pt_render_progressive: frame")) return e;
+    if (pt_status e = s->sum.ensure(3 * px * sizeof(double), "pt_render_progressive: sums")) return e;
+    cudaStream_t stream = s->stream;
+    float* frame = static_cast<float*>(s->out.ptr);
+    double* sum = static_cast<double*>(s->sum.ptr);
+    if (cudaError_t e = cudaMemsetAsync(sum, 0, 3 * px * sizeof(double), stream)) return cuda_fail(e, "render_progressive");
+    if (cudaError_t e = cudaMemsetAsync(s->rays, 0, sizeof(unsigned long long), stream))
+        return cuda_fail(e, "render_progressive");
+    int done = 0, batch = 1;
+    while (done < st->spp) {
+        pt_settings step = *st;
+        step.spp = std::min(batch, st->spp - done);
+        step.first_sample = st->first_sample + done;
+        PtRenderParams p = make_params(cam, &step);
+        p.out = frame;
+        p.rays = s->rays;
+        const auto t0 = std::chrono::steady_clock::now();
+        if (pt_status e = launch_render(s, p, step.mode, stream)) return e;
+        if (pt_status e = pt_accumulate_pass(frame, 3 * px, double(step.spp), sum, stream)) return e;
+        if (pt_status e = read_status(s, stream)) return e;  // waits for the step
+        const double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        done += step.spp;
+        if (ms < 20 && batch < 64)
+            batch *= 2;
+        else if (ms > 60 && batch > 1)
+            batch = std::max(1, batch >> 1);
+        if (progress && done < st->spp && progress(user, done, st->spp) != 0) break;
+    }
+    if (cudaError_t e = pt_launch_mean_of_sum(sum, 3 * px, 1.0 / double(done), frame, stream))
+        return cuda_fail(e, "render_progressive: mean");
+    if (cudaError_t e = cudaMemcpyAsync(out, frame, 3 * px * sizeof(float), cudaMemcpyDeviceToHost, stream))
+        return cuda_fail(e, "render_progressive: output copy");
+    unsigned long long rays = 0;
+    if (cudaError_t e = cudaMemcpyAsync(&rays, s->rays, sizeof(rays), cudaMemcpyDeviceToHost, stream))
+        return cuda_fail(e, "render_progressive: ray count");
+    if (pt_status e = read_status(s, stream)) return e;
+    if (samples_done) *samples_done = done;
     if (rays_out) *rays_out = rays;
     return PT_OK;
 }

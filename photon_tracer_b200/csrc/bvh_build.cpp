@@ -55,6 +55,55 @@ constexpr int kMaxDepth = 64;
 constexpr int kBins = 16;
 constexpr uint32_t kMaxLeaf = 8;
 
+// The 4-wide collapse (include/bvh.hpp:205-242): from the binary root, open
+// the interior child with the largest half area until four children, then
+// recurse into interior children, numbering nodes in that (preorder) order.
+uint32_t collapse_node(const std::vector<BinNode>& bin, uint32_t b, std::vector<pt_bvh_node>& nodes) {
+    uint32_t child[4] = {b, 0, 0, 0};
+    int n = 1;
+    while (n < 4) {
+        int widest = -1;
+        float widest_area = -1;
+        for (int i = 0; i < n; ++i) {
+            const BinNode& c = bin[child[i]];
+            if (c.count == 0 && c.box.half_area() > widest_area) {
+                widest = i;
+                widest_area = c.box.half_area();
+            }
+        }
+        if (widest < 0) break;
+        const uint32_t left = bin[child[widest]].first;
+        child[widest] = left;
+        child[n++] = left + 1;
+    }
+    const uint32_t index = static_cast<uint32_t>(nodes.size());
+    nodes.emplace_back();
+    pt_bvh_node nd;
+    const float inf = std::numeric_limits<float>::infinity();
+    for (int i = 0; i < 4; ++i) {
+        for (int a = 0; a < 3; ++a) {
+            nd.lo[a][i] = i < n ? bin[child[i]].box.mn[a] : inf;
+            nd.hi[a][i] = i < n ? bin[child[i]].box.mx[a] : inf;
+        }
+        nd.first[i] = 0;
+        nd.count[i] = 0;
+        if (i >= n) continue;
+        if (bin[child[i]].count > 0) {
+            nd.first[i] = bin[child[i]].first;
+            nd.count[i] = bin[child[i]].count;
+        } else {
+            nd.first[i] = collapse_node(bin, child[i], nodes);
+        }
+    }
+    nodes[index] = nd;
+    return index;
+}
+
+void collapse_binary(const std::vector<BinNode>& bin, std::vector<pt_bvh_node>& nodes) {
+    nodes.clear();
+    if (!bin.empty()) collapse_node(bin, 0, nodes);
+}
+
 class Builder {
 public:
     Builder(const float* boxes, uint32_t n) : n_(n) {
@@ -77,11 +126,10 @@ public:
         for (uint32_t i = 0; i < n_; ++i) order[i] = i;
         if (n_ == 0) return;
         order_ = &order;
-        nodes_ = &nodes;
         bin_.reserve(2 * size_t(n_));
         bin_.push_back({Box(), 0, n_});
         split(0, 0);
-        collapse(0);
+        collapse_binary(bin_, nodes);
     }
 
 private:
@@ -161,58 +209,28 @@ private:
         split(left + 1, depth + 1);
     }
 
-    uint32_t collapse(uint32_t b) {
-        uint32_t child[4] = {b, 0, 0, 0};
-        int n = 1;
-        while (n < 4) {
-            int widest = -1;
-            float widest_area = -1;
-            for (int i = 0; i < n; ++i) {
-                const BinNode& c = bin_[child[i]];
-                if (c.count == 0 && c.box.half_area() > widest_area) {
-                    widest = i;
-                    widest_area = c.box.half_area();
-                }
-            }
-            if (widest < 0) break;
-            const uint32_t left = bin_[child[widest]].first;
-            child[widest] = left;
-            child[n++] = left + 1;
-        }
-
-        std::vector<pt_bvh_node>& nodes = *nodes_;
-        const uint32_t index = static_cast<uint32_t>(nodes.size());
-        nodes.emplace_back();
-        pt_bvh_node nd;
-        const float inf = std::numeric_limits<float>::infinity();
-        for (int i = 0; i < 4; ++i) {
-            for (int a = 0; a < 3; ++a) {
-                nd.lo[a][i] = i < n ? bin_[child[i]].box.mn[a] : inf;
-                nd.hi[a][i] = i < n ? bin_[child[i]].box.mx[a] : inf;
-            }
-            nd.first[i] = 0;
-            nd.count[i] = 0;
-            if (i >= n) continue;
-            if (bin_[child[i]].count > 0) {
-                nd.first[i] = bin_[child[i]].first;
-                nd.count[i] = bin_[child[i]].count;
-            } else {
-                nd.first[i] = collapse(child[i]);
-            }
-        }
-        nodes[index] = nd;
-        return index;
-    }
-
     uint32_t n_;
     std::vector<Box> prims_;
     std::vector<float> centers_;
     std::vector<BinNode> bin_;
     std::vector<uint32_t>* order_ = nullptr;
-    std::vector<pt_bvh_node>* nodes_ = nullptr;
 };
 
 }  // namespace
+
+void collapse_bvh(const float* boxes, const uint32_t* first, const uint32_t* count, uint32_t n_bin,
+                  std::vector<pt_bvh_node>& nodes) {
+    std::vector<BinNode> bin(n_bin);
+    for (uint32_t i = 0; i < n_bin; ++i) {
+        for (int a = 0; a < 3; ++a) {
+            bin[i].box.mn[a] = boxes[6 * size_t(i) + a];
+            bin[i].box.mx[a] = boxes[6 * size_t(i) + 3 + a];
+        }
+        bin[i].first = first[i];
+        bin[i].count = count[i];
+    }
+    collapse_binary(bin, nodes);
+}
 
 void build_bvh(const float* boxes, uint32_t n, std::vector<pt_bvh_node>& nodes, std::vector<uint32_t>& order) {
     Builder b(boxes, n);

@@ -54,3 +54,6 @@ cudaError_t pt_launch_primary_depth(const PtSceneDev& scene, const PtCamDev& cam
 // of kernel fn that fit on one SM at once, from the device's limits and the
 // kernel's registers and static shared memory.
 int pt_resident_blocks(const void* fn, int threads, size_t dyn_smem);
+
+// out[i] = float(sum[i] * inv): the mean of FP64 per-pixel sums.
+cudaError_t pt_launch_mean_of_sum(const double* sum, size_t n, double inv, float* out, cudaStream_t stream);

@@ -19,6 +19,11 @@ pt_status fail(pt_status code, const std::string& msg);
 
 // ---- BVH and transforms (bvh_build.cpp) -----------------------------------------
 void build_bvh(const float* boxes, uint32_t n, std::vector<pt_bvh_node>& nodes, std::vector<uint32_t>& order);
+// The 4-wide collapse of a binary tree given per binary node its box (6
+// floats), first (left child for interior nodes, leaf start otherwise) and
+// count (0 for interior nodes); node 0 is the root.
+void collapse_bvh(const float* boxes, const uint32_t* first, const uint32_t* count, uint32_t n_bin,
+                  std::vector<pt_bvh_node>& nodes);
 void triangle_box(const float p0[3], const float p1[3], const float p2[3], float out[6]);
 void sphere_box(const float c[3], float r, float out[6]);
 void affine_box(const pt_affine& x, const float in[6], float out[6]);

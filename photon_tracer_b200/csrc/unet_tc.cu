@@ -30,10 +30,18 @@ namespace {
 
 constexpr int kTileX = 16, kTileY = 8, kM = kTileX * kTileY;  // 128 pixels = 128 TMEM lanes
 constexpr int kKc = 32;                                        // input channels per K step (64 bytes)
-constexpr int kStages = 4;
+constexpr int kStagesTile = 4;  // pipeline stages of the shifted-box form
 constexpr int kThreads = 192;  // warp 0: TMA, warp 1: TMEM + MMA, warps 2-5: epilogue
 constexpr uint32_t kABytes = kM * kKc * 2;
 constexpr unsigned long long kWaitNs = 1000000000ull;
+// The halo form (Cout <= 64): an 8 x 16 pixel tile whose 10 x 18 halo box is
+// loaded once per 32 input channels, as four planes of 8 channels (16 bytes
+// per pixel) -- core matrices of 8 pixels x 8 channels -- so the A operand
+// of each tap is the same buffer seen from the tap's offset.
+constexpr int kHaloTX = 8, kHaloTY = 16, kHaloW = kHaloTX + 2, kHaloH = kHaloTY + 2;
+constexpr uint32_t kPlane = kHaloW * kHaloH * 16;  // 2,880 bytes: one 8-channel plane
+constexpr uint32_t kHaloBytes = 4 * kPlane;        // 11,520 bytes per 32 channels
+constexpr uint32_t kHaloStage = 12288;             // rounded up to 1 KB
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
     return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -97,6 +105,23 @@ __device__ __forceinline__ void tma_load_3d(uint32_t dst, const CUtensorMap* map
         : "memory");
 }
 
+__device__ __forceinline__ void tma_load_5d(uint32_t dst, const CUtensorMap* map, int c0, int c1, int c2, int c3,
+                                            int c4, uint32_t bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.5d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, "
+        "%5, %6}], [%7];" ::"r"(dst),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(c4), "r"(bar)
+        : "memory");
+}
+
+// UMMA descriptor of a K-major operand without swizzle: core matrices of
+// 8 rows x 16 bytes stored as 128 contiguous bytes, `lbo` bytes between the
+// two core matrices of a K = 16 step, `sbo` bytes between 8-row groups.
+__device__ __forceinline__ uint64_t plain_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+    return uint64_t((addr >> 4) & 0x3fff) | (uint64_t((lbo >> 4) & 0x3fff) << 16) |
+           (uint64_t((sbo >> 4) & 0x3fff) << 32) | (uint64_t(1) << 46);
+}
+
 // UMMA shared-memory descriptor of a K-major operand with the 64-byte
 // swizzle: rows of 64 bytes, 8-row groups 512 bytes apart (stride byte
 // offset), leading byte offset unused (1), descriptor version 1.
@@ -151,11 +176,11 @@ __device__ __forceinline__ void pack_bf16(const float (&v)[16], uint4& a, uint4&
 }
 
 struct TileGrid {
-    int tiles_x, tiles_y, n;
+    int tiles_x, tiles_y, n, tx, ty;
     __device__ void origin(int t, int& x0, int& y0, int& b) const {
-        x0 = (t % tiles_x) * kTileX;
+        x0 = (t % tiles_x) * tx;
         t /= tiles_x;
-        y0 = (t % tiles_y) * kTileY;
+        y0 = (t % tiles_y) * ty;
         b = t / tiles_y;
     }
 };
@@ -164,33 +189,36 @@ struct TileGrid {
 // TMEM (columns from 0 and from half the allocation, a power of two >= 2N)
 // let the epilogue of one tile overlap the MMAs of the next; the TMA
 // producer runs ahead across tile boundaries.
-template <bool OUT_F32>
+template <bool OUT_F32, bool HALO>
 __global__ void __launch_bounds__(kThreads) conv_tc_kernel(const __grid_constant__ CUtensorMap tm_in,
                                                            const __grid_constant__ CUtensorMap tm_w, int B, int H,
-                                                           int W, int Cin, int N, int tmem_cols,
+                                                           int W, int Cin, int N, int tmem_cols, int stages,
                                                            const float* __restrict__ bias, int relu,
                                                            const unet::ConvOut o, unsigned int* __restrict__ status) {
     extern __shared__ uint8_t smem_raw[];
     uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-    const uint32_t b_bytes = uint32_t(N) * kKc * 2;
+    const uint32_t tap_bytes = uint32_t(N) * kKc * 2;  // one tap's weights for 32 channels
+    const uint32_t a_bytes = HALO ? kHaloStage : kABytes, b_bytes = HALO ? 9 * tap_bytes : tap_bytes;
     uint8_t* sa = smem;
-    uint8_t* sb = smem + kStages * kABytes;
+    uint8_t* sb = smem + stages * a_bytes;
     // full[S], empty[S], acc_full[2], acc_empty[2]
-    uint64_t* bars = reinterpret_cast<uint64_t*>(sb + kStages * b_bytes);
-    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * kStages + 4);
+    uint64_t* bars = reinterpret_cast<uint64_t*>(sb + stages * b_bytes);
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * stages + 4);
     volatile int* abort = reinterpret_cast<volatile int*>(tmem_slot + 1);
-    const uint32_t full0 = smem_u32(bars), empty0 = smem_u32(bars + kStages);
-    const uint32_t acc_full0 = smem_u32(bars + 2 * kStages), acc_empty0 = smem_u32(bars + 2 * kStages + 2);
+    const uint32_t full0 = smem_u32(bars), empty0 = smem_u32(bars + stages);
+    const uint32_t acc_full0 = smem_u32(bars + 2 * stages), acc_empty0 = smem_u32(bars + 2 * stages + 2);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     TileGrid grid;
-    grid.tiles_x = (W + kTileX - 1) / kTileX;
-    grid.tiles_y = (H + kTileY - 1) / kTileY;
+    grid.tx = HALO ? kHaloTX : kTileX;
+    grid.ty = HALO ? kHaloTY : kTileY;
+    grid.tiles_x = (W + grid.tx - 1) / grid.tx;
+    grid.tiles_y = (H + grid.ty - 1) / grid.ty;
     grid.n = grid.tiles_x * grid.tiles_y * B;
-    const int chunks = Cin / kKc, iters = 9 * chunks;
+    const int chunks = Cin / kKc, iters = HALO ? chunks : 9 * chunks;
 
     if (threadIdx.x == 0) {
-        for (int s = 0; s < kStages; ++s) {
+        for (int s = 0; s < stages; ++s) {
             bar_init(full0 + 8 * s, 1);
             bar_init(empty0 + 8 * s, 1);
         }
@@ -222,21 +250,30 @@ __global__ void __launch_bounds__(kThreads) conv_tc_kernel(const __grid_constant
                 int x0, y0, b;
                 grid.origin(t, x0, y0, b);
                 for (int it = 0; it < iters; ++it, ++g) {
-                    const int s = g % kStages;
-                    if (g >= kStages && !wait_bar(empty0 + 8 * s, ((g / kStages) - 1) & 1, abort)) {
+                    const int s = g % stages;
+                    if (g >= stages && !wait_bar(empty0 + 8 * s, ((g / stages) - 1) & 1, abort)) {
                         ok = false;
                         break;
                     }
-                    const int tap = it / chunks, c0 = (it - tap * chunks) * kKc;
-                    bar_expect_tx(full0 + 8 * s, kABytes + b_bytes);
-                    tma_load_4d(smem_u32(sa + s * kABytes), &tm_in, c0, x0 + tap % 3 - 1, y0 + tap / 3 - 1, b,
-                                full0 + 8 * s);
-                    tma_load_3d(smem_u32(sb + s * b_bytes), &tm_w, c0, tap, 0, full0 + 8 * s);
+                    if (HALO) {
+                        // the halo box of 32 channels (4 planes), and the 9 taps' weights for them
+                        const int c0 = it * kKc;
+                        bar_expect_tx(full0 + 8 * s, kHaloBytes + b_bytes);
+                        tma_load_5d(smem_u32(sa + s * a_bytes), &tm_in, 0, x0 - 1, y0 - 1, c0 / 8, b, full0 + 8 * s);
+                        for (int tap = 0; tap < 9; ++tap)
+                            tma_load_3d(smem_u32(sb + s * b_bytes + tap * tap_bytes), &tm_w, c0, tap, 0, full0 + 8 * s);
+                    } else {
+                        const int tap = it / chunks, c0 = (it - tap * chunks) * kKc;
+                        bar_expect_tx(full0 + 8 * s, kABytes + b_bytes);
+                        tma_load_4d(smem_u32(sa + s * a_bytes), &tm_in, c0, x0 + tap % 3 - 1, y0 + tap / 3 - 1, b,
+                                    full0 + 8 * s);
+                        tma_load_3d(smem_u32(sb + s * b_bytes), &tm_w, c0, tap, 0, full0 + 8 * s);
+                    }
                 }
             }
             // The copies issued into each stage have landed before the CTA can exit.
-            for (int k = g > kStages ? g - kStages : 0; k < g; ++k)
-                if (!wait_bar(full0 + 8 * (k % kStages), (k / kStages) & 1, nullptr)) ok = false;
+            for (int k = g > stages ? g - stages : 0; k < g; ++k)
+                if (!wait_bar(full0 + 8 * (k % stages), (k / stages) & 1, nullptr)) ok = false;
         }
     } else if (warp == 1) {
         if (lane == 0) {
@@ -254,17 +291,31 @@ __global__ void __launch_bounds__(kThreads) conv_tc_kernel(const __grid_constant
                 fence_after();
                 const uint32_t d = tmem + uint32_t(a * (tmem_cols / 2));
                 for (int it = 0; it < iters; ++it, ++g) {
-                    const int s = g % kStages;
-                    if (!wait_bar(full0 + 8 * s, (g / kStages) & 1, abort)) {
+                    const int s = g % stages;
+                    if (!wait_bar(full0 + 8 * s, (g / stages) & 1, abort)) {
                         ok = false;
                         break;
                     }
                     fence_after();
-                    const uint64_t ad = sw64_desc(smem_u32(sa + s * kABytes));
-                    const uint64_t bd = sw64_desc(smem_u32(sb + s * b_bytes));
+                    if (HALO) {
+                        // tap (dy, dx) reads the halo from offset (dy + 1, dx + 1): 8-pixel
+                        // rows 10 pixels apart (SBO 160 B), K planes 2,880 B apart (LBO)
+                        const uint32_t a0 = smem_u32(sa + s * a_bytes), b0 = smem_u32(sb + s * b_bytes);
+                        for (int tap = 0; tap < 9; ++tap) {
+                            const uint32_t off = uint32_t((tap / 3) * kHaloW + tap % 3) * 16u;
+                            const uint64_t bd = sw64_desc(b0 + tap * tap_bytes);
 #pragma unroll
-                    for (int k = 0; k < kKc / 16; ++k)  // K = 16 per MMA: +32 bytes along the row
-                        mma_bf16(d, ad + uint64_t(2 * k), bd + uint64_t(2 * k), idesc, (it | k) != 0);
+                            for (int k = 0; k < kKc / 16; ++k)
+                                mma_bf16(d, plain_desc(a0 + 2 * k * kPlane + off, kPlane, kHaloW * 16),
+                                         bd + uint64_t(2 * k), idesc, (it | tap | k) != 0);
+                        }
+                    } else {
+                        const uint64_t ad = sw64_desc(smem_u32(sa + s * a_bytes));
+                        const uint64_t bd = sw64_desc(smem_u32(sb + s * b_bytes));
+#pragma unroll
+                        for (int k = 0; k < kKc / 16; ++k)  // K = 16 per MMA: +32 bytes along the row
+                            mma_bf16(d, ad + uint64_t(2 * k), bd + uint64_t(2 * k), idesc, (it | k) != 0);
+                    }
                     mma_commit(empty0 + 8 * s);
                 }
                 mma_commit(acc_full0 + 8 * a);
@@ -283,13 +334,14 @@ __global__ void __launch_bounds__(kThreads) conv_tc_kernel(const __grid_constant
             fence_after();
             int x0, y0, b;
             grid.origin(t, x0, y0, b);
-            const int px = x0 + (m % kTileX), py = y0 + (m / kTileX);
+            const int px = x0 + (m % grid.tx), py = y0 + (m / grid.tx);
             const bool valid = px < W && py < H;
             const size_t pix = (size_t(b) * H + (valid ? py : 0)) * W + (valid ? px : 0);
-            // Pooling windows: lanes 0-15 hold tile row 2q, lanes 16-31 row
-            // 2q + 1 (x0, y0 even), so a window is lanes {l, l^1, l^16, l^17}
-            // and its even-x lane of the upper row writes it.
-            const bool pool_writer = valid && !(lane & 17);
+            // Pooling windows (x0, y0 even): the x neighbour is lane ^ 1, the
+            // y neighbour lane ^ tx (a warp holds 32 / tx whole tile rows);
+            // the even-x lane of the even row writes the window.
+            const int ylane = HALO ? 8 : 16;
+            const bool pool_writer = valid && !(lane & (1 | ylane));
             const size_t ppix = (size_t(b) * (H >> 1) + (py >> 1)) * (W >> 1) + (px >> 1);
             for (int c = 0; c < N; c += 16) {
                 float v[16];
@@ -337,7 +389,7 @@ __global__ void __launch_bounds__(kThreads) conv_tc_kernel(const __grid_constant
 #pragma unroll
                     for (int j = 0; j < 16; ++j) {
                         v[j] = fmaxf(v[j], __shfl_xor_sync(0xffffffffu, v[j], 1));
-                        v[j] = fmaxf(v[j], __shfl_xor_sync(0xffffffffu, v[j], 16));
+                        v[j] = fmaxf(v[j], __shfl_xor_sync(0xffffffffu, v[j], ylane));
                     }
                     if (pool_writer) {
                         uint4 p0, p1;
@@ -380,7 +432,17 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
     return fn;
 }
 
-size_t smem_bytes(int N) { return 1024 + kStages * (kABytes + size_t(N) * kKc * 2) + (2 * kStages + 4) * 8 + 8; }
+// Pipeline stages and dynamic shared memory of the two forms.
+int conv_stages(bool halo, int N) { return halo ? (N <= 32 ? 3 : 2) : kStagesTile; }
+size_t smem_bytes(bool halo, int N) {
+    const int st = conv_stages(halo, N);
+    const size_t a = halo ? kHaloStage : kABytes, b = (halo ? 9 : 1) * size_t(N) * kKc * 2;
+    const size_t need = 1024 + st * (a + b) + (2 * st + 4) * 8 + 8;
+    // The halo form reads its A operand through descriptors with 2,880-byte
+    // strides; the allocation keeps 96 KB beyond the first stage so that no
+    // descriptor reach can leave it.
+    return halo ? std::max<size_t>(need, 1024 + 98304 + 128) : need;
+}
 
 // CTAs that fit on all SMs at once: the kernel's resident blocks per SM
 // (shared memory, threads, registers), capped by the TMEM columns each holds.
@@ -558,8 +620,24 @@ cudaError_t conv_fwd_tc(const ConvShape& s, const __nv_bfloat16* in, const __nv_
     PFN_cuTensorMapEncodeTiled_v12000 encode = encode_fn();
     if (!encode) return cudaErrorNotSupported;
 
+    // The halo form for Cout <= 64 (where re-reading the shifted box per tap
+    // bounds the kernel), the shifted-box form otherwise or if the halo's
+    // tensor map is refused.
+    bool halo = N <= 64;
     CUtensorMap tm_in, tm_w;
-    {
+    if (halo) {
+        // [B][H][W][Cin] seen as (8 channels, x, y, channel group, image): the
+        // box (8, 10, 18, 4, 1) lands as four 8-channel planes of the halo.
+        const cuuint64_t dims[5] = {8, cuuint64_t(s.W), cuuint64_t(s.H), cuuint64_t(s.Cin / 8), cuuint64_t(s.B)};
+        const cuuint64_t strides[4] = {cuuint64_t(s.Cin) * 2, cuuint64_t(s.W) * s.Cin * 2, 16,
+                                       cuuint64_t(s.H) * s.W * s.Cin * 2};
+        const cuuint32_t box[5] = {8, kHaloW, kHaloH, 4, 1};
+        const cuuint32_t estr[5] = {1, 1, 1, 1, 1};
+        halo = encode(&tm_in, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 5, const_cast<__nv_bfloat16*>(in), dims, strides, box,
+                      estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                      CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+    }
+    if (!halo) {
         const cuuint64_t dims[4] = {cuuint64_t(s.Cin), cuuint64_t(s.W), cuuint64_t(s.H), cuuint64_t(s.B)};
         const cuuint64_t strides[3] = {cuuint64_t(s.Cin) * 2, cuuint64_t(s.W) * s.Cin * 2,
                                        cuuint64_t(s.H) * s.W * s.Cin * 2};
@@ -582,21 +660,34 @@ cudaError_t conv_fwd_tc(const ConvShape& s, const __nv_bfloat16* in, const __nv_
     }
     int cols = 32;
     while (cols < 2 * N) cols *= 2;  // two accumulators
-    const size_t smem = smem_bytes(N);
-    const long tiles = long((s.W + kTileX - 1) / kTileX) * ((s.H + kTileY - 1) / kTileY) * s.B;
+    const size_t smem = smem_bytes(halo, N);
+    const int stages = conv_stages(halo, N);
+    const int tx = halo ? kHaloTX : kTileX, ty = halo ? kHaloTY : kTileY;
+    const long tiles = long((s.W + tx - 1) / tx) * ((s.H + ty - 1) / ty) * s.B;
     if (tiles > 0x7fffffffL) return cudaErrorNotSupported;
-    const void* fn = out_f32 ? reinterpret_cast<const void*>(conv_tc_kernel<true>)
-                             : reinterpret_cast<const void*>(conv_tc_kernel<false>);
+    const void* fn = out_f32 ? (halo ? reinterpret_cast<const void*>(conv_tc_kernel<true, true>)
+                                     : reinterpret_cast<const void*>(conv_tc_kernel<true, false>))
+                             : (halo ? reinterpret_cast<const void*>(conv_tc_kernel<false, true>)
+                                     : reinterpret_cast<const void*>(conv_tc_kernel<false, false>));
     cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
     if (e) return e;
     const long g = grid_size(cols, smem, fn);
     const unsigned blocks = unsigned(tiles < g ? tiles : g);
-    if (out_f32)
-        conv_tc_kernel<true><<<blocks, kThreads, smem, st>>>(tm_in, tm_w, s.B, s.H, s.W, s.Cin, N, cols, bias, relu, o,
-                                                             status);
-    else
-        conv_tc_kernel<false><<<blocks, kThreads, smem, st>>>(tm_in, tm_w, s.B, s.H, s.W, s.Cin, N, cols, bias, relu, o,
-                                                              status);
+#define PT_CONV_LAUNCH(F32, HALO)                                                                                     \
+    conv_tc_kernel<F32, HALO><<<blocks, kThreads, smem, st>>>(tm_in, tm_w, s.B, s.H, s.W, s.Cin, N, cols, stages, bias, \
+                                                             relu, o, status)
+    if (out_f32) {
+        if (halo)
+            PT_CONV_LAUNCH(true, true);
+        else
+            PT_CONV_LAUNCH(true, false);
+    } else {
+        if (halo)
+            PT_CONV_LAUNCH(false, true);
+        else
+            PT_CONV_LAUNCH(false, false);
+    }
+#undef PT_CONV_LAUNCH
     return cudaGetLastError();
 }
 

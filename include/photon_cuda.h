@@ -64,7 +64,17 @@ typedef struct pt_material {
     float emission[3];
     float fuzz;
     float ior;
+    uint32_t texture; /* lambertian::texture (:50): 0 for none, k for pt_scene_desc.textures[k - 1]
+                         (so a zeroed material has none); the albedo is then multiplied by the
+                         texture at the hit's texture coordinates */
 } pt_material;
+
+/* An image texture (include/texture.hpp:9-48): width x height texels of sRGB
+ * bytes, 3 per texel, rows top first (the image8 the reference decodes). */
+typedef struct pt_texture {
+    int32_t width, height;
+    const uint8_t* rgb;
+} pt_texture;
 
 /* A sphere: include/sphere.hpp:15-17. A negative radius is a hollow shell. */
 typedef struct pt_sphere {
@@ -85,6 +95,7 @@ typedef struct pt_triangle {
     float face_normal[3];
     float p1[3], p2[3];
     uint32_t material;
+    float uv[6];  /* texture coordinates at the three corners (include/triangle.hpp:20) */
 } pt_triangle;
 
 /* A 3x3 + translation affine transform: include/transform.hpp:11-12. */
@@ -155,6 +166,8 @@ typedef struct pt_scene_desc {
     int32_t sky;           /* geometry::sky (:30) */
     int32_t sample_lights; /* geometry::sample_lights (:32), next event estimation */
     int32_t use_bvh;       /* geometry::build(use_bvh) (:74) */
+    const pt_texture* textures; /* the images textured lambertians refer to */
+    uint32_t n_textures;
 } pt_scene_desc;
 
 typedef struct pt_scene pt_scene;
@@ -441,7 +454,8 @@ enum {
     PT_GEN_RANDOM_SPHERES = 10, /* 22x22 random spheres + ground + light, seed */
     PT_GEN_ROOM_MESH = 11,      /* closed room + displaced icosphere (subdivisions = param) */
     PT_GEN_INSTANCES = 12,      /* 10,000 instances of three procedural meshes */
-    PT_GEN_BATCH_SCENE = 13     /* one scene of the 64-scene batch, by seed */
+    PT_GEN_BATCH_SCENE = 13,    /* one scene of the 64-scene batch, by seed */
+    PT_GEN_TEXTURED = 14        /* the room with textured walls, sphere and instanced meshes, seed */
 };
 typedef struct pt_gen_params {
     int32_t kind;

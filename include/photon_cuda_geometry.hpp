@@ -14,7 +14,9 @@
 //   if (gpu.upload(world) != PT_OK) fail(pt_last_error());
 //   gpu.render(cam, W, H, spp, 10, image.data(), seed, 0, aux_or_null, &rays);
 //
-// Textures (lambertian::texture) are not carried: the GPU path has none.
+// Textured lambertians carry their texture's sRGB image (texture.hpp) and
+// the triangles their texture coordinates; the desc points into the
+// geometry's own images, so the geometry must outlive the upload.
 #pragma once
 
 #include <cstring>
@@ -48,11 +50,27 @@ struct scene_arrays {
     std::vector<pt_mesh> meshes;
     std::vector<pt_instance> instances;
     std::vector<uint32_t> lights;
+    std::vector<pt_texture> textures;  // point into the geometry's textures (kept alive by it)
     pt_scene_desc desc;
 
     // Fills the arrays and desc from a built geometry.
     void from(const geometry& world) {
         std::map<const material*, uint32_t> index;
+        std::map<const image_texture*, uint32_t> tex_index;
+        // a texture's sRGB image, once per texture (lambertian::texture, texture.hpp:36-38);
+        // materials refer to textures[k] as k + 1
+        auto tex = [&](const image_texture* t) -> uint32_t {
+            auto found = tex_index.find(t);
+            if (found != tex_index.end()) return found->second;
+            pt_texture pt;
+            pt.width = t->source.width;
+            pt.height = t->source.height;
+            pt.rgb = t->source.rgb.data();
+            const uint32_t k = uint32_t(textures.size()) + 1;
+            textures.push_back(pt);
+            tex_index.emplace(t, k);
+            return k;
+        };
         auto mat = [&](const material* m) -> uint32_t {
             if (!m) return PT_NO_MATERIAL;
             auto found = index.find(m);
@@ -60,9 +78,11 @@ struct scene_arrays {
             pt_material p;
             std::memset(&p, 0, sizeof(p));
             p.ior = 1.5f;
+            p.texture = 0;
             if (auto* l = dynamic_cast<const lambertian*>(m)) {
                 p.type = PT_MAT_LAMBERTIAN;
                 for (int a = 0; a < 3; ++a) p.albedo[a] = l->albedo.e[a];
+                if (l->texture) p.texture = tex(l->texture.get());
             } else if (auto* me = dynamic_cast<const metal*>(m)) {
                 p.type = PT_MAT_METAL;
                 for (int a = 0; a < 3; ++a) p.albedo[a] = me->albedo.e[a];
@@ -93,6 +113,7 @@ struct scene_arrays {
             for (int k = 0; k < 9; ++k)
                 for (int a = 0; a < 3; ++a) dst[k][a] = src[k]->e[a];
             p.material = mat(t.mat);
+            for (int k = 0; k < 6; ++k) p.uv[k] = t.uv[k];
             return p;
         };
         auto tree = [](const bvh& b) {
@@ -154,6 +175,8 @@ struct scene_arrays {
         desc.n_lights = uint32_t(lights.size());
         desc.sky = world.sky ? 1 : 0;
         desc.sample_lights = world.sample_lights ? 1 : 0;
+        desc.textures = textures.data();
+        desc.n_textures = uint32_t(textures.size());
     }
 };
 

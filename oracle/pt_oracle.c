@@ -61,6 +61,7 @@ typedef struct po_scene {
     tree* mesh;
     uint32_t* lights;
     uint32_t n_lights;
+    float** texels; /* per texture: linear RGB (image_texture's texels, texture.hpp:13-21) */
 } po_scene;
 
 static int emits(const pt_material* m) { return m->emission[0] > 0 || m->emission[1] > 0 || m->emission[2] > 0; }
@@ -85,6 +86,22 @@ po_scene* po_scene_create(const pt_scene_desc* d, const pt_bvh* flat, const pt_b
         s->mesh[i].n_nodes = meshes[i].n_nodes;
         s->mesh[i].order = meshes[i].order;
     }
+    /* image_texture (texture.hpp:13-21): sRGB bytes to linear through a 256-entry table */
+    s->texels = (float**)calloc(d->n_textures ? d->n_textures : 1, sizeof(float*));
+    if (d->n_textures) {
+        float table[256];
+        int v;
+        for (v = 0; v < 256; ++v) {
+            const float c = v / 255.0f;
+            table[v] = c <= 0.04045f ? c / 12.92f : powf((c + 0.055f) / 1.055f, 2.4f);
+        }
+        for (i = 0; i < d->n_textures; ++i) {
+            const size_t n = 3 * (size_t)d->textures[i].width * (size_t)d->textures[i].height;
+            size_t k;
+            s->texels[i] = (float*)malloc((n ? n : 1) * sizeof(float));
+            for (k = 0; k < n; ++k) s->texels[i][k] = table[d->textures[i].rgb[k]];
+        }
+    }
     /* geometry::build's light list (geometry.hpp:75-77) */
     s->lights = (uint32_t*)calloc(d->n_spheres ? d->n_spheres : 1, sizeof(uint32_t));
     if (d->lights) {
@@ -98,7 +115,10 @@ po_scene* po_scene_create(const pt_scene_desc* d, const pt_bvh* flat, const pt_b
 }
 
 void po_scene_destroy(po_scene* s) {
+    uint32_t i;
     if (!s) return;
+    for (i = 0; i < s->d.n_textures; ++i) free(s->texels[i]);
+    free(s->texels);
     free(s->mesh);
     free(s->lights);
     free(s);
@@ -414,6 +434,7 @@ typedef struct {
     float t;
     int front_face, sampled_light;
     uint32_t mat;
+    float tex_u, tex_v;
 } rec_t;
 
 static void fill_sphere(const pt_sphere* s, v3 o, v3 d, float t, rec_t* r) {
@@ -434,6 +455,27 @@ static void fill_triangle(const pt_triangle* tr, v3 o, v3 d, float t, float u, f
     n = normalize(add(add(scl(ld3(tr->n0), 1 - u - v), scl(ld3(tr->n1), u)), scl(ld3(tr->n2), v)));
     r->normal = r->front_face ? n : neg(n);
     r->mat = tr->material;
+    r->tex_u = tr->uv[0] * (1 - u - v) + tr->uv[2] * u + tr->uv[4] * v;
+    r->tex_v = tr->uv[1] * (1 - u - v) + tr->uv[3] * u + tr->uv[5] * v;
+}
+
+/* image_texture::sample (texture.hpp:25-33) */
+static v3 texel(const po_scene* s, uint32_t k, int x, int y) {
+    const int w = s->d.textures[k].width, h = s->d.textures[k].height;
+    const float* t;
+    x = ((x % w) + w) % w;
+    y = ((y % h) + h) % h;
+    t = &s->texels[k][3 * ((size_t)y * w + x)];
+    return mk(t[0], t[1], t[2]);
+}
+static v3 sample_texture(const po_scene* s, uint32_t k, float u, float v) {
+    const float x = (u - floorf(u)) * (float)s->d.textures[k].width - 0.5f;
+    const float y = (1 - (v - floorf(v))) * (float)s->d.textures[k].height - 0.5f;
+    const int x0 = (int)floorf(x), y0 = (int)floorf(y);
+    const float fx = x - (float)x0, fy = y - (float)y0;
+    return add(add(add(scl(texel(s, k, x0, y0), (1 - fx) * (1 - fy)), scl(texel(s, k, x0 + 1, y0), fx * (1 - fy))),
+                   scl(texel(s, k, x0, y0 + 1), (1 - fx) * fy)),
+               scl(texel(s, k, x0 + 1, y0 + 1), fx * fy));
 }
 
 static int hit(const po_scene* s, v3 o, v3 d, float t_min, float t_max, rec_t* r, counts* cnt) {
@@ -441,6 +483,8 @@ static int hit(const po_scene* s, v3 o, v3 d, float t_min, float t_max, rec_t* r
     hctx c;
     closest(s, o, d, t_min, &t_max, &c, cnt);
     r->sampled_light = 0;
+    r->tex_u = 0;
+    r->tex_v = 0;
     switch (c.kind) {
         case PT_HIT_LARGE: fill_sphere(&D->large_spheres[c.index], o, d, t_max, r); return 1;
         case PT_HIT_SPHERE:
@@ -714,6 +758,8 @@ static v3 ray_color(const po_scene* s, v3 o, v3 d, int depth, sampler_t* q, rng_
         m = &s->d.materials[rec.mat];
         if (rec.front_face && !(sampled && rec.sampled_light)) rad = add(rad, mul(tp, ld3(m->emission)));
         scatters = scatter(m, d, &rec, q, r, &att, &dir);
+        /* lambertian: albedo * texture->sample(tex_u, tex_v) (material.hpp:72) */
+        if (m->type == PT_MAT_LAMBERTIAN && m->texture > 0) att = mul(att, sample_texture(s, m->texture - 1, rec.tex_u, rec.tex_v));
         if (bounce == 0) {
             *f_albedo = scatters && m->type != PT_MAT_DIELECTRIC ? att : mk(1, 1, 1);
             *f_normal = rec.normal;

@@ -27,10 +27,21 @@ struct ref_scene {
     std::vector<const material*> mats;
 };
 
-std::shared_ptr<material> material_from(const pt_material& m) {
+// The reference's own image_texture over a pt_texture's sRGB bytes.
+std::shared_ptr<const image_texture> texture_from(const pt_texture& t) {
+    image8 img;
+    img.width = t.width;
+    img.height = t.height;
+    img.rgb.assign(t.rgb, t.rgb + 3 * size_t(t.width) * size_t(t.height));
+    return std::make_shared<const image_texture>(img);
+}
+
+std::shared_ptr<material> material_from(const pt_material& m,
+                                        const std::vector<std::shared_ptr<const image_texture>>& textures) {
     const color albedo(m.albedo[0], m.albedo[1], m.albedo[2]);
     switch (m.type) {
-        case PT_MAT_LAMBERTIAN: return std::make_shared<lambertian>(albedo);
+        case PT_MAT_LAMBERTIAN:
+            return std::make_shared<lambertian>(albedo, m.texture > 0 ? textures[m.texture - 1] : nullptr);
         case PT_MAT_METAL: return std::make_shared<metal>(albedo, m.fuzz);
         case PT_MAT_DIELECTRIC: return std::make_shared<dielectric>(m.ior);
         default: return std::make_shared<diffuse_light>(color(m.emission[0], m.emission[1], m.emission[2]));
@@ -41,7 +52,9 @@ point3 P(const float* p) { return point3(p[0], p[1], p[2]); }
 
 triangle make_tri(const pt_triangle& t, const material* m) {
     // The reference's smooth constructor from the corners as given.
-    return triangle(P(t.p0), P(t.p1), P(t.p2), P(t.n0), P(t.n1), P(t.n2), m);
+    triangle tr(P(t.p0), P(t.p1), P(t.p2), P(t.n0), P(t.n1), P(t.n2), m);
+    for (int k = 0; k < 6; ++k) tr.uv[k] = t.uv[k];
+    return tr;
 }
 
 // The camera with its four fields set (the reference's constructor fixes the
@@ -68,7 +81,9 @@ extern "C" {
 void* ref_scene_create(const pt_scene_desc* d) {
     auto* s = new ref_scene();
     geometry& w = s->world;
-    for (uint32_t i = 0; i < d->n_materials; ++i) s->mats.push_back(w.own(material_from(d->materials[i])));
+    std::vector<std::shared_ptr<const image_texture>> textures;
+    for (uint32_t k = 0; k < d->n_textures; ++k) textures.push_back(texture_from(d->textures[k]));
+    for (uint32_t i = 0; i < d->n_materials; ++i) s->mats.push_back(w.own(material_from(d->materials[i], textures)));
     for (uint32_t i = 0; i < d->n_spheres; ++i) {
         const pt_sphere& sp = d->spheres[i];
         w.spheres.emplace_back(P(sp.center), sp.radius, s->mats[sp.material]);

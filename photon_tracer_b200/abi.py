@@ -41,12 +41,18 @@ PT_GEN_RANDOM_SPHERES = 10
 PT_GEN_ROOM_MESH = 11
 PT_GEN_INSTANCES = 12
 PT_GEN_BATCH_SCENE = 13
+PT_GEN_TEXTURED = 14
 
 F3 = C.c_float * 3
 
 
 class pt_material(C.Structure):
-    _fields_ = [("type", C.c_uint32), ("albedo", F3), ("emission", F3), ("fuzz", C.c_float), ("ior", C.c_float)]
+    _fields_ = [("type", C.c_uint32), ("albedo", F3), ("emission", F3), ("fuzz", C.c_float), ("ior", C.c_float),
+                ("texture", C.c_uint32)]
+
+
+class pt_texture(C.Structure):
+    _fields_ = [("width", C.c_int32), ("height", C.c_int32), ("rgb", C.POINTER(C.c_uint8))]
 
 
 class pt_sphere(C.Structure):
@@ -55,7 +61,7 @@ class pt_sphere(C.Structure):
 
 class pt_triangle(C.Structure):
     _fields_ = [("p0", F3), ("e1", F3), ("e2", F3), ("n0", F3), ("n1", F3), ("n2", F3), ("face_normal", F3),
-                ("p1", F3), ("p2", F3), ("material", C.c_uint32)]
+                ("p1", F3), ("p2", F3), ("material", C.c_uint32), ("uv", C.c_float * 6)]
 
 
 class pt_affine(C.Structure):
@@ -89,7 +95,8 @@ class pt_scene_desc(C.Structure):
                 ("instances", C.POINTER(pt_instance)), ("n_instances", C.c_uint32),
                 ("flat_tree", pt_bvh), ("instance_tree", pt_bvh),
                 ("lights", C.POINTER(C.c_uint32)), ("n_lights", C.c_uint32),
-                ("sky", C.c_int32), ("sample_lights", C.c_int32), ("use_bvh", C.c_int32)]
+                ("sky", C.c_int32), ("sample_lights", C.c_int32), ("use_bvh", C.c_int32),
+                ("textures", C.POINTER(pt_texture)), ("n_textures", C.c_uint32)]
 
 
 class pt_scene_info(C.Structure):
@@ -236,13 +243,13 @@ def f3(v) -> "C.Array":
 
 TRIANGLE_DTYPE = np.dtype([("p0", "<f4", 3), ("e1", "<f4", 3), ("e2", "<f4", 3), ("n0", "<f4", 3), ("n1", "<f4", 3),
                            ("n2", "<f4", 3), ("face_normal", "<f4", 3), ("p1", "<f4", 3), ("p2", "<f4", 3),
-                           ("material", "<u4")])
+                           ("material", "<u4"), ("uv", "<f4", 6)])
 SPHERE_DTYPE = np.dtype([("center", "<f4", 3), ("radius", "<f4"), ("material", "<u4")])
 AFFINE_DTYPE = np.dtype([("m", "<f4", (3, 3)), ("t", "<f4", 3)])
 INSTANCE_DTYPE = np.dtype([("mesh", "<u4"), ("material", "<u4"), ("to_world", AFFINE_DTYPE),
                            ("to_object", AFFINE_DTYPE)])
 MATERIAL_DTYPE = np.dtype([("type", "<u4"), ("albedo", "<f4", 3), ("emission", "<f4", 3), ("fuzz", "<f4"),
-                           ("ior", "<f4")])
+                           ("ior", "<f4"), ("texture", "<u4")])
 assert TRIANGLE_DTYPE.itemsize == C.sizeof(pt_triangle)
 assert SPHERE_DTYPE.itemsize == C.sizeof(pt_sphere)
 assert INSTANCE_DTYPE.itemsize == C.sizeof(pt_instance)

@@ -235,7 +235,8 @@ pt_status pt_scene_create(const pt_scene_desc* desc, pt_scene** out) {
                          align256(A.large.size() * sizeof(float4)) + align256(A.large_mat.size() * 4) +
                          align256(A.sph.size() * sizeof(PtShadeSphere)) + align256(A.tri.size() * sizeof(PtShadeTri)) +
                          align256(A.inst.size() * sizeof(PtShadeInst)) + align256(A.mat.size() * sizeof(PtMaterial)) +
-                         align256(A.lights.size() * sizeof(PtLight)) + 3 * 256;
+                         align256(A.lights.size() * sizeof(PtLight)) + align256(A.tri_uv.size() * 4) +
+                         align256(A.tex.size() * sizeof(int4)) + align256(A.texels.size() * 4) + 3 * 256;
     cudaError_t err = cudaMalloc(&s->arena, bytes);
     if (err != cudaSuccess) {
         delete s;
@@ -255,6 +256,10 @@ pt_status pt_scene_create(const pt_scene_desc* desc, pt_scene** out) {
     D.inst = upload(base, off, A.inst, err);
     D.mat = upload(base, off, A.mat, err);
     D.lights = upload(base, off, A.lights, err);
+    D.tri_uv = upload(base, off, A.tri_uv, err);
+    D.tex = upload(base, off, A.tex, err);
+    D.texels = upload(base, off, A.texels, err);
+    D.has_textures = A.has_textures;
     s->status = reinterpret_cast<unsigned int*>(base + off);
     off += 256;
     s->work = reinterpret_cast<unsigned int*>(base + off);

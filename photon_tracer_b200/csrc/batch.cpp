@@ -89,7 +89,8 @@ PtBatchScene merge(HostArena& dst, const HostArena& src) {
                    islot_base = uint32_t(dst.islots.size() / 16), sph_base = uint32_t(dst.sph.size()),
                    tri_base = uint32_t(dst.tri.size()), inst_base = uint32_t(dst.inst.size()),
                    mat_base = uint32_t(dst.mat.size()), large_base = uint32_t(dst.large.size()),
-                   light_base = uint32_t(dst.lights.size());
+                   light_base = uint32_t(dst.lights.size()), tex_base = uint32_t(dst.tex.size()),
+                   texel_base = uint32_t(dst.texels.size());
     const float inf = std::numeric_limits<float>::infinity();
     for (size_t n = 0; n < src.nodes.size(); n += 32) {
         float rec[32];
@@ -137,8 +138,19 @@ PtBatchScene merge(HostArena& dst, const HostArena& src) {
         if (in.material != PT_NONE) in.material += mat_base;
         dst.inst.push_back(in);
     }
-    dst.mat.insert(dst.mat.end(), src.mat.begin(), src.mat.end());
+    for (PtMaterial m : src.mat) {
+        const uint32_t t = bitsf(m.ior_flags.z);
+        if (t != PT_NONE) m.ior_flags.z = ubits(t + tex_base);
+        dst.mat.push_back(m);
+    }
     dst.lights.insert(dst.lights.end(), src.lights.begin(), src.lights.end());
+    dst.tri_uv.insert(dst.tri_uv.end(), src.tri_uv.begin(), src.tri_uv.end());
+    for (int4 t : src.tex) {
+        t.z += int(texel_base);
+        dst.tex.push_back(t);
+    }
+    dst.texels.insert(dst.texels.end(), src.texels.begin(), src.texels.end());
+    dst.has_textures |= src.has_textures;
     PtBatchScene b;
     std::memset(&b, 0, sizeof(b));
     b.flat_root = src.flat_root == PT_NONE ? PT_NONE : src.flat_root + node_base;
@@ -360,7 +372,9 @@ pt_status pt_batch_create(const pt_batch_item* items, uint32_t n, int32_t strate
                          align256(all.large.size() * sizeof(float4)) + align256(all.large_mat.size() * 4) +
                          align256(all.sph.size() * sizeof(PtShadeSphere)) + align256(all.tri.size() * sizeof(PtShadeTri)) +
                          align256(all.inst.size() * sizeof(PtShadeInst)) + align256(all.mat.size() * sizeof(PtMaterial)) +
-                         align256(all.lights.size() * sizeof(PtLight)) + align256(n * sizeof(PtBatchScene)) +
+                         align256(all.lights.size() * sizeof(PtLight)) + align256(all.tri_uv.size() * 4) +
+                         align256(all.tex.size() * sizeof(int4)) + align256(all.texels.size() * 4) +
+                         align256(n * sizeof(PtBatchScene)) +
                          align256(out_floats * 4) + align256(n * 4) + align256(n * 8) + 4 * 256;
     cudaError_t err = cudaMalloc(&b->arena, bytes);
     if (err) return cuda_fail(err, "pt_batch_create: device allocation");
@@ -379,6 +393,10 @@ pt_status pt_batch_create(const pt_batch_item* items, uint32_t n, int32_t strate
     D.inst = upload(base, off, all.inst, err);
     D.mat = upload(base, off, all.mat, err);
     D.lights = upload(base, off, all.lights, err);
+    D.tri_uv = upload(base, off, all.tri_uv, err);
+    D.tex = upload(base, off, all.tex, err);
+    D.texels = upload(base, off, all.texels, err);
+    D.has_textures = all.has_textures;
     b->d_scenes = upload(base, off, b->scenes, err);
     b->d_out = reinterpret_cast<float*>(base + off);
     off += align256(out_floats * 4);

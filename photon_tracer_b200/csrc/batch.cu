@@ -33,7 +33,7 @@ __device__ __forceinline__ unsigned long long global_ns() {
 #define PT_BATCH_MIN_BLOCKS128 3
 #endif
 
-template <int THREADS, int TREES>
+template <int THREADS, int TREES, bool TEX>
 __global__ void __launch_bounds__(THREADS, PT_BATCH_MIN_BLOCKS128 * 128 / THREADS)
     batch_megakernel(PtSceneDev S0, PtBatchLaunch B) {
     StackEntry stack[PT_STACK_MAX];
@@ -143,10 +143,10 @@ __global__ void __launch_bounds__(THREADS, PT_BATCH_MIN_BLOCKS128 * 128 / THREAD
                 h.kind = PT_HIT_NONE;
             }
             const bool hit = h.kind != PT_HIT_NONE;
-            if (hit) fill(S, h, path.o, path.d, t, rec);
+            if (hit) fill<TEX>(S, h, path.o, path.d, t, rec);
             bool nee;
             Shadow sh;
-            const int step = shade<false>(S, path, hit, rec, depth, smp, rng, first, nee, sh, rays);
+            const int step = shade<false, TEX>(S, path, hit, rec, depth, smp, rng, first, nee, sh, rays);
             if (nee) {
                 bool ovf = false;
                 if (!occluded<false, TREES>(S, sh.o, sh.d, 0.001f, sh.t_max, stack, cnt, &ovf)) path.rad = path.rad + sh.value;
@@ -177,34 +177,42 @@ __global__ void __launch_bounds__(THREADS, PT_BATCH_MIN_BLOCKS128 * 128 / THREAD
     if (__any_sync(0xffffffffu, overflow) && lane == 0) atomicOr(S0.status, PT_DEV_ERR_STACK);
 }
 
-template <int THREADS, int TREES>
+template <int THREADS, int TREES, bool TEX>
 void launch(const PtSceneDev& S, const PtBatchLaunch& b, int sms, cudaStream_t stream) {
-    const int blocks = pt_resident_blocks(reinterpret_cast<const void*>(batch_megakernel<THREADS, TREES>), THREADS, 0);
-    batch_megakernel<THREADS, TREES><<<sms * blocks, THREADS, 0, stream>>>(S, b);
+    const int blocks =
+        pt_resident_blocks(reinterpret_cast<const void*>(batch_megakernel<THREADS, TREES, TEX>), THREADS, 0);
+    batch_megakernel<THREADS, TREES, TEX><<<sms * blocks, THREADS, 0, stream>>>(S, b);
 }
 
-template <int TREES>
+template <int TREES, bool TEX>
 void launch_threads(const PtSceneDev& S, const PtBatchLaunch& b, int threads, int sms, cudaStream_t stream) {
     switch (threads) {
         case 64:
-            launch<64, TREES>(S, b, sms, stream);
+            launch<64, TREES, TEX>(S, b, sms, stream);
             break;
         case 256:
-            launch<256, TREES>(S, b, sms, stream);
+            launch<256, TREES, TEX>(S, b, sms, stream);
             break;
         default:
-            launch<128, TREES>(S, b, sms, stream);
+            launch<128, TREES, TEX>(S, b, sms, stream);
             break;
     }
 }
 
 }  // namespace
 
-// The single-loop traversal when some scene has instances, one loop per tree otherwise.
+// The single-loop traversal when some scene has instances, one loop per tree
+// otherwise; texture code only when some scene has textures.
 cudaError_t pt_launch_batch(const PtSceneDev& S, const PtBatchLaunch& b, int threads, int sms, cudaStream_t stream) {
-    if (b.any_instances)
-        launch_threads<PT_TREES_ONE>(S, b, threads, sms, stream);
-    else
-        launch_threads<PT_TREES_EACH>(S, b, threads, sms, stream);
+    if (S.has_textures) {
+        if (b.any_instances)
+            launch_threads<PT_TREES_ONE, true>(S, b, threads, sms, stream);
+        else
+            launch_threads<PT_TREES_EACH, true>(S, b, threads, sms, stream);
+    } else if (b.any_instances) {
+        launch_threads<PT_TREES_ONE, false>(S, b, threads, sms, stream);
+    } else {
+        launch_threads<PT_TREES_EACH, false>(S, b, threads, sms, stream);
+    }
     return cudaGetLastError();
 }

@@ -576,6 +576,12 @@ __global__ void small_kernel(Prims P, const LNode* __restrict__ roots, uint32_t 
     }
 }
 
+// Empty keys: minima all ones, maxima zero (q % 6 < 3 are minima in both key arrays).
+__global__ void init_keys_kernel(unsigned long long* __restrict__ keys, size_t n) {
+    for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x)
+        keys[i] = (i % 6) < 3 ? kEmptyMin : kEmptyMax;
+}
+
 struct TreeUpdate {
     uint32_t idx, first, count;
 };
@@ -685,14 +691,14 @@ cudaError_t build_device(const float* h_boxes, uint32_t n, std::vector<float>& b
         if (!e) e = d_cb.ensure(L);
         if (!e) e = d_ce.ensure(L);
         if (e) break;
-        // Empty keys: min keys all ones, max keys zero (the same layout in both arrays: q % 6 < 3 are minima).
-        std::vector<unsigned long long> init_keys(12 * size_t(L)), init_bins(size_t(kBinKeys) * L);
-        for (size_t q = 0; q < init_keys.size(); ++q) init_keys[q] = (q % 6) < 3 ? kEmptyMin : kEmptyMax;
-        for (size_t q = 0; q < init_bins.size(); ++q) init_bins[q] = (q % 6) < 3 ? kEmptyMin : kEmptyMax;
         e = cudaMemcpyAsync(d_nodes.p, level.data(), L * sizeof(LNode), cudaMemcpyHostToDevice, st);
         if (!e) e = cudaMemcpyAsync(d_chunks.p, chunks.data(), C * sizeof(Chunk), cudaMemcpyHostToDevice, st);
-        if (!e) e = cudaMemcpyAsync(d_keys.p, init_keys.data(), init_keys.size() * 8, cudaMemcpyHostToDevice, st);
-        if (!e) e = cudaMemcpyAsync(d_bin_keys.p, init_bins.data(), init_bins.size() * 8, cudaMemcpyHostToDevice, st);
+        if (!e) {
+            init_keys_kernel<<<std::min<size_t>((12 * size_t(L) + 255) / 256, 1184), 256, 0, st>>>(d_keys.p, 12 * size_t(L));
+            init_keys_kernel<<<std::min<size_t>((size_t(kBinKeys) * L + 255) / 256, 1184), 256, 0, st>>>(
+                d_bin_keys.p, size_t(kBinKeys) * L);
+            e = cudaGetLastError();
+        }
         if (!e) e = cudaMemsetAsync(d_bin_count.p, 0, 3 * kBins * size_t(L) * 4, st);
         if (!e) e = cudaMemcpyAsync(d_cb.p, cbeg.data(), L * 4, cudaMemcpyHostToDevice, st);
         if (!e) e = cudaMemcpyAsync(d_ce.p, cend.data(), L * 4, cudaMemcpyHostToDevice, st);

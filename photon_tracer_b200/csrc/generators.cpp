@@ -30,6 +30,8 @@ struct pt_generated {
     std::vector<std::vector<pt_triangle>> mesh_tris;
     std::vector<pt_mesh> meshes;
     std::vector<pt_instance> instances;
+    std::vector<std::vector<uint8_t>> images;  // sRGB bytes of the textures
+    std::vector<pt_texture> textures;
     pt_scene_desc desc;
     pt_camera cam;
 };
@@ -77,10 +79,22 @@ struct SceneBuilder {
         store(m.emission, emission);
         m.fuzz = fuzz;
         m.ior = ior;
+        m.texture = 0;
         g->materials.push_back(m);
         return static_cast<uint32_t>(g->materials.size() - 1);
     }
     uint32_t lambertian(V3 a) { return material(PT_MAT_LAMBERTIAN, a, V3{0, 0, 0}, 0, 1.5f); }
+    uint32_t textured(V3 a, uint32_t texture) {
+        const uint32_t m = lambertian(a);
+        g->materials[m].texture = texture;
+        return m;
+    }
+    // A texture of w x h sRGB texels; returns its 1-based number for materials.
+    uint32_t texture(int w, int h, std::vector<uint8_t> rgb) {
+        g->images.push_back(std::move(rgb));
+        g->textures.push_back({w, h, nullptr});
+        return uint32_t(g->textures.size());
+    }
     // metal(a, f): fuzz(f < 1 ? f : 1) (include/material.hpp:83)
     uint32_t metal(V3 a, float f) { return material(PT_MAT_METAL, a, V3{0, 0, 0}, f < 1 ? f : 1, 1.5f); }
     uint32_t dielectric(float ior) { return material(PT_MAT_DIELECTRIC, V3{0, 0, 0}, V3{0, 0, 0}, 0, ior); }
@@ -466,8 +480,89 @@ void instances_scene(SceneBuilder& b, uint64_t seed, int n_instances) {
     }
 }
 
+// A textured scene (no counterpart among the reference's scenes; it exercises
+// lambertian::texture, include/material.hpp:50-72): the reference's room
+// with seeded sRGB checker textures on the floor and the back wall, a
+// textured sphere (texture coordinates (0, 0), as sphere::fill leaves them),
+// and six instances of an icosphere with longitude/latitude coordinates,
+// every other one with a textured override material.
+void textured_scene(SceneBuilder& b, uint64_t seed) {
+    pt_generated* g = b.g;
+    std::mt19937 rng(static_cast<uint32_t>(seed));
+    auto u = [&rng] { return rng() * 0x1.0p-32; };
+    auto checker = [&](int w, int h, int cells) {
+        std::vector<uint8_t> rgb(3 * size_t(w) * h);
+        std::vector<uint8_t> cell(3 * cells * cells);
+        for (auto& c : cell) c = uint8_t(40 + 215 * u());
+        for (int y = 0; y < h; ++y)
+            for (int x = 0; x < w; ++x)
+                for (int c = 0; c < 3; ++c) {
+                    const int cx = x * cells / w, cy = y * cells / h;
+                    rgb[3 * (size_t(y) * w + x) + c] = uint8_t((cell[3 * (cy * cells + cx) + c] + 7 * ((x + y) & 7)) & 255);
+                }
+        return rgb;
+    };
+    const uint32_t floor_tex = b.texture(96, 64, checker(96, 64, 8));
+    const uint32_t wall_tex = b.texture(37, 53, checker(37, 53, 5));
+    g->desc.sky = 0;
+    const uint32_t white = b.lambertian(p3(0.73, 0.73, 0.73));
+    const uint32_t red = b.lambertian(p3(0.65, 0.05, 0.05));
+    const uint32_t green = b.lambertian(p3(0.12, 0.45, 0.15));
+    const uint32_t floor_mat = b.textured(p3(0.9, 0.9, 0.9), floor_tex);
+    const uint32_t wall_mat = b.textured(p3(0.8, 0.8, 0.8), wall_tex);
+    const double x0 = -1.75, x1 = 1.75, y0 = -1, y1 = 1, z0 = -3.5, z1 = 0.5;
+    // a quad with texture coordinates (0,0) (r,0) (r,r) (0,r) at p, p+e1, p+e1+e2, p+e2
+    auto tquad = [&](V3 p, V3 e1, V3 e2, uint32_t m, float r) {
+        pt_triangle a = make_triangle(p, p + e1, p + e1 + e2, m), c = make_triangle(p, p + e1 + e2, p + e2, m);
+        const float ua[6] = {0, 0, r, 0, r, r}, uc[6] = {0, 0, r, r, 0, r};
+        std::memcpy(a.uv, ua, sizeof(ua));
+        std::memcpy(c.uv, uc, sizeof(uc));
+        g->triangles.push_back(a);
+        g->triangles.push_back(c);
+    };
+    tquad(p3(x0, y0, z1), p3(x1 - x0, 0, 0), p3(0, 0, z0 - z1), floor_mat, 2.5f);  // floor, repeating
+    b.quad(p3(x0, y1, z1), p3(x1 - x0, 0, 0), p3(0, 0, z0 - z1), white);          // ceiling
+    tquad(p3(x0, y0, z0), p3(x1 - x0, 0, 0), p3(0, y1 - y0, 0), wall_mat, 1.0f);  // back
+    b.quad(p3(x0, y0, z1), p3(x1 - x0, 0, 0), p3(0, y1 - y0, 0), white);          // front
+    b.quad(p3(x0, y0, z1), p3(0, 0, z0 - z1), p3(0, y1 - y0, 0), red);            // left
+    b.quad(p3(x1, y0, z1), p3(0, 0, z0 - z1), p3(0, y1 - y0, 0), green);          // right
+    b.sphere(p3(0, 0.72, -2.0), 0.14f, b.light(p3(30, 27, 22)));
+    b.sphere(p3(0.15, -0.75, -2.9), 0.25f, b.textured(p3(1, 1, 1), wall_tex));
+
+    Mesh ico = icosphere(3);
+    std::vector<pt_triangle> tris = smooth_triangles(ico, b.textured(p3(0.95, 0.95, 0.95), floor_tex));
+    for (size_t f = 0; f < ico.f.size(); ++f)
+        for (int k = 0; k < 3; ++k) {
+            const auto& v = ico.v[ico.f[f][k]];
+            tris[f].uv[2 * k] = float(std::atan2(v[2], v[0]) / (2 * M_PI) + 0.5);
+            tris[f].uv[2 * k + 1] = float(std::asin(std::max(-1.0, std::min(1.0, v[1]))) / M_PI + 0.5);
+        }
+    g->mesh_tris.push_back(tris);
+    for (int k = 0; k < 6; ++k) {
+        const double s = 0.18 + 0.1 * u(), yaw = 2 * M_PI * u();
+        pt_affine w;
+        std::memset(&w, 0, sizeof(w));
+        const double c = std::cos(yaw), sn = std::sin(yaw);
+        const double R[3][3] = {{c, 0, sn}, {0, 1, 0}, {-sn, 0, c}};
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j) w.m[i][j] = float(R[i][j] * s);
+        w.t[0] = float(-1.2 + 0.5 * k);
+        w.t[1] = float(-1 + s);
+        w.t[2] = float(-1.6 - 0.25 * (k % 3));
+        pt_instance in;
+        in.mesh = 0;
+        in.material = (k % 2) ? b.textured(p3(0.7 + 0.3 * u(), 0.7, 0.7), wall_tex) : PT_NO_MATERIAL;
+        in.to_world = w;
+        in.to_object = affine_inverse(w);
+        g->instances.push_back(in);
+    }
+}
+
 void finish(pt_generated* g) {
     pt_scene_desc& d = g->desc;
+    for (size_t k = 0; k < g->textures.size(); ++k) g->textures[k].rgb = g->images[k].data();
+    d.textures = g->textures.data();
+    d.n_textures = uint32_t(g->textures.size());
     g->meshes.clear();
     for (auto& t : g->mesh_tris) {
         pt_mesh m;
@@ -563,6 +658,11 @@ pt_status pt_generate(pt_gen_params* params, pt_generated** out) {
             instances_scene(b, params->seed, params->param > 0 ? params->param : 10000);
             store(from, p3(0, 35, 140)); store(at, p3(0, 0, 0)); vfov = 45.0;
             width = 1920; height = 1080; spp = 32;
+            break;
+        case PT_GEN_TEXTURED:
+            textured_scene(b, params->seed);
+            store(from, p3(0, 0, 0.3)); store(at, p3(0, -0.15, -3.0)); vfov = 62.0;
+            width = 960; height = 540; spp = 200;
             break;
         case PT_GEN_BATCH_SCENE: {
             // One scene of the 64-scene batch: the random-spheres generator

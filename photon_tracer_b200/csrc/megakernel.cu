@@ -25,7 +25,7 @@ constexpr int kTileW = 8, kTileH = 4;
 #define PT_MEGA_MIN_BLOCKS 3
 #endif
 
-template <bool AUX, bool SNAP, int TREES>
+template <bool AUX, bool SNAP, int TREES, bool TEX>
 __global__ void __launch_bounds__(128, PT_MEGA_MIN_BLOCKS) megakernel(PtSceneDev S, PtRenderParams P, uint32_t tiles_x,
                                                   uint32_t total_items) {
     StackEntry stack[PT_STACK_MAX];
@@ -123,10 +123,10 @@ __global__ void __launch_bounds__(128, PT_MEGA_MIN_BLOCKS) megakernel(PtSceneDev
                 h.kind = PT_HIT_NONE;
             }
             const bool hit = h.kind != PT_HIT_NONE;
-            if (hit) fill(S, h, path.o, path.d, t, rec);
+            if (hit) fill<TEX>(S, h, path.o, path.d, t, rec);
             bool nee;
             Shadow sh;
-            const int step = shade<AUX>(S, path, hit, rec, P.depth, smp, rng, first, nee, sh, rays);
+            const int step = shade<AUX, TEX>(S, path, hit, rec, P.depth, smp, rng, first, nee, sh, rays);
             if (nee) {
                 bool ovf = false;
                 if (!occluded<false, TREES>(S, sh.o, sh.d, 0.001f, sh.t_max, stack, cnt, &ovf))
@@ -174,45 +174,54 @@ __global__ void __launch_bounds__(128, PT_MEGA_MIN_BLOCKS) megakernel(PtSceneDev
     if (__any_sync(0xffffffffu, overflow) && lane == 0) atomicOr(S.status, PT_DEV_ERR_STACK);
 }
 
-template <bool AUX, bool SNAP, int TREES>
+template <bool AUX, bool SNAP, int TREES, bool TEX>
 cudaError_t launch(const PtSceneDev& S, const PtRenderParams& p, const PtLaunchShape& shape, cudaStream_t stream) {
     const uint32_t tiles_x = uint32_t((p.width + kTileW - 1) / kTileW);
     const uint32_t tiles_y = uint32_t((p.rows + kTileH - 1) / kTileH);
     const uint32_t total = tiles_x * tiles_y * 32u;
-    megakernel<AUX, SNAP, TREES><<<shape.blocks, shape.threads, 0, stream>>>(S, p, tiles_x, total);
+    megakernel<AUX, SNAP, TREES, TEX><<<shape.blocks, shape.threads, 0, stream>>>(S, p, tiles_x, total);
     return cudaGetLastError();
 }
 
-template <int TREES>
-cudaError_t launch_trees(const PtSceneDev& S, const PtRenderParams& p, const PtLaunchShape& shape,
-                         cudaStream_t stream) {
+template <int TREES, bool TEX>
+cudaError_t launch_form(const PtSceneDev& S, const PtRenderParams& p, const PtLaunchShape& shape,
+                        cudaStream_t stream) {
     const bool aux = p.aux != nullptr, snap = p.rng_mode == 1;
     if (aux)
-        return snap ? launch<true, true, TREES>(S, p, shape, stream) : launch<true, false, TREES>(S, p, shape, stream);
-    return snap ? launch<false, true, TREES>(S, p, shape, stream) : launch<false, false, TREES>(S, p, shape, stream);
+        return snap ? launch<true, true, TREES, TEX>(S, p, shape, stream)
+                    : launch<true, false, TREES, TEX>(S, p, shape, stream);
+    return snap ? launch<false, true, TREES, TEX>(S, p, shape, stream)
+                : launch<false, false, TREES, TEX>(S, p, shape, stream);
 }
 
-template <int TREES>
+template <int TREES, bool TEX>
 int occupancy(int threads, bool aux, bool snap) {
-    const void* fn = aux ? (snap ? reinterpret_cast<const void*>(megakernel<true, true, TREES>)
-                                 : reinterpret_cast<const void*>(megakernel<true, false, TREES>))
-                         : (snap ? reinterpret_cast<const void*>(megakernel<false, true, TREES>)
-                                 : reinterpret_cast<const void*>(megakernel<false, false, TREES>));
+    const void* fn = aux ? (snap ? reinterpret_cast<const void*>(megakernel<true, true, TREES, TEX>)
+                                 : reinterpret_cast<const void*>(megakernel<true, false, TREES, TEX>))
+                         : (snap ? reinterpret_cast<const void*>(megakernel<false, true, TREES, TEX>)
+                                 : reinterpret_cast<const void*>(megakernel<false, false, TREES, TEX>));
     return pt_resident_blocks(fn, threads, 0);
 }
 
-// The single-loop traversal for scenes with instances, one loop per tree otherwise.
+// The single-loop traversal for scenes with instances, one loop per tree
+// otherwise; texture code only in the kernels for scenes with textures.
 bool one_loop(const PtSceneDev& S) { return S.use_bvh && S.inst_root != PT_NONE; }
 
 }  // namespace
 
 cudaError_t pt_launch_megakernel(const PtSceneDev& S, const PtRenderParams& p, const PtLaunchShape& shape,
                                  cudaStream_t stream) {
-    return one_loop(S) ? launch_trees<PT_TREES_ONE>(S, p, shape, stream)
-                       : launch_trees<PT_TREES_EACH>(S, p, shape, stream);
+    if (S.has_textures)
+        return one_loop(S) ? launch_form<PT_TREES_ONE, true>(S, p, shape, stream)
+                           : launch_form<PT_TREES_EACH, true>(S, p, shape, stream);
+    return one_loop(S) ? launch_form<PT_TREES_ONE, false>(S, p, shape, stream)
+                       : launch_form<PT_TREES_EACH, false>(S, p, shape, stream);
 }
 
 int pt_megakernel_blocks_per_sm(const PtSceneDev& S, int threads, bool aux, bool snapshot) {
-    return one_loop(S) ? occupancy<PT_TREES_ONE>(threads, aux, snapshot)
-                       : occupancy<PT_TREES_EACH>(threads, aux, snapshot);
+    if (S.has_textures)
+        return one_loop(S) ? occupancy<PT_TREES_ONE, true>(threads, aux, snapshot)
+                           : occupancy<PT_TREES_EACH, true>(threads, aux, snapshot);
+    return one_loop(S) ? occupancy<PT_TREES_ONE, false>(threads, aux, snapshot)
+                       : occupancy<PT_TREES_EACH, false>(threads, aux, snapshot);
 }

@@ -88,7 +88,7 @@ enum : int { STEP_CONTINUE = 0, STEP_DONE = 1 };
 // record (or a miss). Sets *nee and sh when a shadow ray must be tested, with
 // sh.value already multiplied by throughput * attenuation; the caller adds it
 // to p.rad if the ray is not blocked. Returns STEP_DONE when the path ends.
-template <bool AUX>
+template <bool AUX, bool TEX = true>
 __device__ __forceinline__ int shade(const PtSceneDev& S, Path& p, bool hit, const Rec& rec, int depth,
                                      const Sampler& smp, Rng& rng, First& first, bool& nee, Shadow& sh,
                                      unsigned long long& rays) {
@@ -108,6 +108,10 @@ __device__ __forceinline__ int shade(const PtSceneDev& S, Path& p, bool hit, con
     if (rec.front_face && !(p.sampled && rec.sampled_light)) p.rad = p.rad + p.tp * xyz(ef);
     V att, dir;
     const bool scatters = scatter(mat, type, p.d, rec, smp, rng, att, dir);
+    if (TEX && S.has_textures && type == PT_MAT_LAMBERTIAN) {  // albedo * texture->sample(tex_u, tex_v) (:72)
+        const uint32_t tex = fbits(mat.ior_flags.z);
+        if (tex != PT_NONE) att = att * sample_texture(S, tex, rec.tex_u, rec.tex_v);
+    }
     if (AUX && p.bounce == 0)
         first = {scatters && !(flags & PT_MF_TRANSMISSIVE) ? att : mk(1, 1, 1), rec.normal};
     if (!scatters) return STEP_DONE;

@@ -49,7 +49,7 @@
 struct PtMaterial {   // 48 B
     float4 albedo_type;   // albedo.xyz, type (as float bits of uint)
     float4 emission_fuzz; // emission.xyz, fuzz
-    float4 ior_flags;     // ior, flags (bits), 0, 0
+    float4 ior_flags;     // ior, flags (bits), texture (bits; PT_NONE: none), 0
 };
 
 struct PtShadeTri {   // 64 B
@@ -89,6 +89,9 @@ struct PtSceneDev {
     const PtShadeInst* inst;
     const PtMaterial* mat;
     const PtLight* lights;
+    const float* tri_uv;      // 6 per shading triangle: texture coordinates at the corners
+    const int4* tex;          // per texture: width, height, first texel float, 0
+    const float* texels;      // linear RGB, 3 floats per texel, rows top first
     unsigned int* status;     // device error word
     uint32_t flat_root;       // PT_NONE when there is no flat tree
     uint32_t inst_root;
@@ -98,4 +101,5 @@ struct PtSceneDev {
     uint32_t n_lights;
     uint32_t n_spheres;       // top-level spheres
     int sky, sample_lights, use_bvh;
+    int has_textures;         // some lambertian has a texture
 };

@@ -8,6 +8,8 @@
 // exactly as geometry::build would (include/geometry.hpp:74-104).
 #include "scene_host.hpp"
 
+#include <cmath>
+
 #include <algorithm>
 #include <cstring>
 #include <limits>
@@ -98,6 +100,20 @@ void push_tri_shade(HostArena& A, const pt_triangle& t) {
     s.n2 = make_float4(t.n2[0], t.n2[1], t.n2[2], 0);
     s.fn = make_float4(t.face_normal[0], t.face_normal[1], t.face_normal[2], 0);
     A.tri.push_back(s);
+    A.tri_uv.insert(A.tri_uv.end(), t.uv, t.uv + 6);
+}
+
+// image_texture's constructor (include/texture.hpp:13-21): sRGB bytes to
+// linear floats through the same 256-entry table, std::pow in float.
+void decode_texture(const pt_texture& t, HostArena& A) {
+    float table[256];
+    for (int v = 0; v < 256; ++v) {
+        const float c = v / 255.0f;
+        table[v] = c <= 0.04045f ? c / 12.92f : std::pow((c + 0.055f) / 1.055f, 2.4f);
+    }
+    const size_t n = 3 * size_t(t.width) * size_t(t.height);
+    A.tex.push_back(make_int4(t.width, t.height, int(A.texels.size()), 0));
+    for (size_t k = 0; k < n; ++k) A.texels.push_back(table[t.rgb[k]]);
 }
 
 }  // namespace
@@ -113,6 +129,16 @@ pt_status build_arena(const pt_scene_desc& d, HostArena& A) {
         return fail(PT_ERR_INVALID_ARG, "scene: too many primitives");
     for (uint32_t i = 0; i < nm; ++i)
         if (d.materials[i].type > PT_MAT_DIFFUSE_LIGHT) return fail(PT_ERR_INVALID_ARG, "material: unknown type");
+    if (d.n_textures && !d.textures) return fail(PT_ERR_INVALID_ARG, "textures: null pointer");
+    uint64_t texels = 0;
+    for (uint32_t k = 0; k < d.n_textures; ++k) {
+        const pt_texture& t = d.textures[k];
+        if (t.width <= 0 || t.height <= 0 || !t.rgb) return fail(PT_ERR_INVALID_ARG, "texture: empty or null image");
+        texels += uint64_t(t.width) * uint64_t(t.height);
+    }
+    if (texels > (1ull << 28)) return fail(PT_ERR_INVALID_ARG, "textures: more than 2^28 texels");
+    for (uint32_t i = 0; i < nm; ++i)
+        if (d.materials[i].texture > d.n_textures) return fail(PT_ERR_INVALID_ARG, "material: texture out of range");
     auto mat_ok = [&](uint32_t m) { return m < nm; };
     for (uint32_t i = 0; i < d.n_spheres; ++i)
         if (!mat_ok(d.spheres[i].material)) return fail(PT_ERR_INVALID_ARG, "sphere: material out of range");
@@ -146,9 +172,13 @@ pt_status build_arena(const pt_scene_desc& d, HostArena& A) {
         PtMaterial g;
         g.albedo_type = make_float4(m.albedo[0], m.albedo[1], m.albedo[2], ubits(m.type));
         g.emission_fuzz = make_float4(m.emission[0], m.emission[1], m.emission[2], m.fuzz);
-        g.ior_flags = make_float4(m.ior, ubits(flags), 0, 0);
+        // only lambertians are textured (lambertian::texture, include/material.hpp:50)
+        const bool textured = m.type == PT_MAT_LAMBERTIAN && m.texture > 0;
+        g.ior_flags = make_float4(m.ior, ubits(flags), ubits(textured ? m.texture - 1 : PT_NONE), 0);
+        A.has_textures |= textured ? 1 : 0;
         A.mat.push_back(g);
     }
+    for (uint32_t k = 0; k < d.n_textures; ++k) decode_texture(d.textures[k], A);
 
     // Lights: given, or every emissive sphere (include/geometry.hpp:75-77).
     std::vector<uint32_t> lights;

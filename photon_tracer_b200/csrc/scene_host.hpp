@@ -22,6 +22,10 @@ struct HostArena {
     std::vector<PtShadeInst> inst;
     std::vector<PtMaterial> mat;
     std::vector<PtLight> lights;
+    std::vector<float> tri_uv;    // 6 per shading triangle
+    std::vector<int4> tex;        // width, height, first texel float, 0
+    std::vector<float> texels;    // linear RGB
+    int has_textures = 0;
     uint32_t flat_root = PT_NONE, inst_root = PT_NONE;
     uint32_t n_flat_slots = 0, n_instances = 0, n_spheres = 0;
     uint32_t stack_entries = 0, max_depth = 0;

@@ -742,6 +742,7 @@ struct Rec {
     bool front_face;
     bool sampled_light;
     uint32_t mat;
+    float tex_u, tex_v;  // texture coordinates (only filled in scenes with textures)
 };
 
 // sphere::fill (include/sphere.hpp:50-58)
@@ -755,21 +756,50 @@ __device__ __forceinline__ void fill_sphere(float4 cr, uint32_t mat, V o, V d, f
 }
 
 // triangle::fill (include/triangle.hpp:63-74), direction d in the triangle's space.
-__device__ __forceinline__ void fill_triangle(const PtShadeTri* __restrict__ tri, uint32_t g, V d, float u, float v,
-                                              Rec& rec) {
+template <bool TEX>
+__device__ __forceinline__ void fill_triangle(const PtSceneDev& S, uint32_t g, V d, float u, float v, Rec& rec) {
+    const PtShadeTri* __restrict__ tri = S.tri;
     const float4 a = __ldg(&tri[g].n0_mat), b = __ldg(&tri[g].n1), c = __ldg(&tri[g].n2), f = __ldg(&tri[g].fn);
     rec.front_face = dot(d, xyz(f)) < 0;
     const float w = 1 - u - v;
     const V n = normalize(xyz(a) * w + xyz(b) * u + xyz(c) * v);
     rec.normal = rec.front_face ? n : -n;
     rec.mat = fbits(a.w);
+    if (TEX && S.has_textures) {  // rec.tex_u, tex_v (:72-73)
+        const float* q = S.tri_uv + 6 * size_t(g);
+        rec.tex_u = __ldg(q) * w + __ldg(q + 2) * u + __ldg(q + 4) * v;
+        rec.tex_v = __ldg(q + 1) * w + __ldg(q + 3) * u + __ldg(q + 5) * v;
+    }
+}
+
+// image_texture::sample (include/texture.hpp:25-33): bilinear, repeating
+// outside [0, 1), v up the image while rows are stored top first.
+__device__ __forceinline__ V texel(const PtSceneDev& S, int4 t, int x, int y) {
+    x = ((x % t.x) + t.x) % t.x;
+    y = ((y % t.y) + t.y) % t.y;
+    const float* p = S.texels + size_t(uint32_t(t.z)) + 3 * (size_t(y) * size_t(t.x) + size_t(x));
+    return mk(__ldg(p), __ldg(p + 1), __ldg(p + 2));
+}
+__device__ __forceinline__ V sample_texture(const PtSceneDev& S, uint32_t k, float u, float v) {
+    const int4 t = __ldg(S.tex + k);
+    const float x = (u - floorf(u)) * float(t.x) - 0.5f;
+    const float y = (1 - (v - floorf(v))) * float(t.y) - 0.5f;
+    const int x0 = static_cast<int>(floorf(x)), y0 = static_cast<int>(floorf(y));
+    const float fx = x - float(x0), fy = y - float(y0);
+    return texel(S, t, x0, y0) * ((1 - fx) * (1 - fy)) + texel(S, t, x0 + 1, y0) * (fx * (1 - fy)) +
+           texel(S, t, x0, y0 + 1) * ((1 - fx) * fy) + texel(S, t, x0 + 1, y0 + 1) * (fx * fy);
 }
 
 // The record geometry::hit fills for the nearest primitive (:141-151,
 // fill_instance :234-244).
+// TEX = false compiles out the texture coordinates (kernels for scenes
+// without textures: two fewer live registers through the shading code).
+template <bool TEX = true>
 __device__ __forceinline__ void fill(const PtSceneDev& S, const Hit& h, V o, V d, float t, Rec& rec) {
     rec.sampled_light = false;
     rec.t = t;
+    rec.tex_u = 0;
+    rec.tex_v = 0;
     switch (h.kind) {
         case PT_HIT_LARGE:
             fill_sphere(__ldg(S.large + h.index), __ldg(S.large_mat + h.index), o, d, t, rec);
@@ -785,7 +815,7 @@ __device__ __forceinline__ void fill(const PtSceneDev& S, const Hit& h, V o, V d
         case PT_HIT_TRIANGLE: {
             const uint32_t i = fbits(__ldg(S.slots + 3 * size_t(h.index) + 2).y);
             rec.p = o + d * t;
-            fill_triangle(S.tri, i, d, h.u, h.v, rec);
+            fill_triangle<TEX>(S, i, d, h.u, h.v, rec);
             break;
         }
         case PT_HIT_INSTANCE: {
@@ -794,7 +824,7 @@ __device__ __forceinline__ void fill(const PtSceneDev& S, const Hit& h, V o, V d
             const uint32_t tri_base = __ldg(&in->tri_base), over = __ldg(&in->material);
             const uint32_t sub = fbits(__ldg(S.slots + 3 * size_t(h.index) + 2).y);
             const V ld = aff_vector(rows, d);
-            fill_triangle(S.tri, tri_base + sub, ld, h.u, h.v, rec);
+            fill_triangle<TEX>(S, tri_base + sub, ld, h.u, h.v, rec);
             rec.p = o + d * t;
             rec.normal = normalize(aff_transposed(rows, rec.normal));
             if (over != PT_NONE) rec.mat = over;

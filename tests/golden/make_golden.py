@@ -48,6 +48,7 @@ RENDER_CASES = [
     ("random_spheres", abi.PT_GEN_RANDOM_SPHERES, 0, 40, 23, 2),
     ("ref_field", abi.PT_GEN_REF_FIELD, 0, 40, 23, 2),
     ("instances", abi.PT_GEN_INSTANCES, 400, 32, 18, 1),
+    ("textured", abi.PT_GEN_TEXTURED, 0, 48, 27, 2),
 ]
 TREE_CASES = [("ref_materials", abi.PT_GEN_REF_MATERIALS, 0), ("ref_field", abi.PT_GEN_REF_FIELD, 0),
               ("ref_room", abi.PT_GEN_REF_ROOM, 0), ("random_spheres", abi.PT_GEN_RANDOM_SPHERES, 0),

@@ -43,12 +43,14 @@ def test_struct_sizes_match_c(built, tmp_path):
     from photon_tracer_b200 import abi
     structs = ["pt_material", "pt_sphere", "pt_triangle", "pt_affine", "pt_bvh_node", "pt_bvh", "pt_mesh",
                "pt_instance", "pt_scene_desc", "pt_scene_info", "pt_camera", "pt_settings", "pt_hit", "pt_gen_params",
-               "pt_batch_item", "pt_batch_info"]
+               "pt_batch_item", "pt_batch_info", "pt_texture"]
     src = tmp_path / "sizes.c"
     src.write_text('#include <stdio.h>\n#include <stddef.h>\n#include "photon_cuda.h"\nint main(void){\n' +
                    "".join(f'printf("{s} %zu\\n", sizeof({s}));\n' for s in structs) +
                    'printf("off_settings_states %zu\\n", offsetof(pt_settings, rng_states));\n'
-                   'printf("off_desc_use_bvh %zu\\n", offsetof(pt_scene_desc, use_bvh));\nreturn 0;}\n')
+                   'printf("off_desc_use_bvh %zu\\n", offsetof(pt_scene_desc, use_bvh));\n'
+                   'printf("off_desc_textures %zu\\n", offsetof(pt_scene_desc, textures));\n'
+                   'printf("off_tri_uv %zu\\n", offsetof(pt_triangle, uv));\nreturn 0;}\n')
     exe = tmp_path / "sizes"
     subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
     out = dict(line.split() for line in subprocess.run([str(exe)], capture_output=True, text=True).stdout.splitlines())
@@ -56,6 +58,8 @@ def test_struct_sizes_match_c(built, tmp_path):
         assert int(out[s]) == C.sizeof(getattr(abi, s)), s
     assert int(out["off_settings_states"]) == abi.pt_settings.rng_states.offset
     assert int(out["off_desc_use_bvh"]) == abi.pt_scene_desc.use_bvh.offset
+    assert int(out["off_desc_textures"]) == abi.pt_scene_desc.textures.offset
+    assert int(out["off_tri_uv"]) == abi.pt_triangle.uv.offset
 
 
 def test_version_and_error_text(built):

@@ -15,7 +15,7 @@ def pt(built):
 
 
 def small_batch(pt):
-    """Mixed scenes at small sizes: batch-generator scenes plus instances and the reference room."""
+    """Mixed scenes at small sizes: batch-generator scenes plus instances, the reference room and two textured rooms."""
     from photon_tracer_b200 import abi
     items = []
     for s in (3, 7, 12, 21):
@@ -25,6 +25,9 @@ def small_batch(pt):
     items.append((g, g.camera, 64, 36, 2, 5))
     g = pt.Generated(abi.PT_GEN_REF_ROOM)
     items.append((g, g.camera, 50, 30, 3, 9))
+    for s in (4, 5):  # textures: their numbers and texel offsets are rebased in the merged arena
+        g = pt.Generated(abi.PT_GEN_TEXTURED, seed=s)
+        items.append((g, g.camera, 56, 32, 2, 30 + s))
     return items
 
 

@@ -67,7 +67,7 @@ def test_snapshot_render_matches_reference(pt, name):
 
 @pytest.mark.parametrize("kind,param,w,h,spp", [
     ("ROOM_MESH", 6, 64, 64, 4), ("RANDOM_SPHERES", 0, 80, 45, 4), ("INSTANCES", 0, 64, 36, 2),
-    ("REF_ROOM", 0, 64, 36, 4), ("REF_MATERIALS", 0, 64, 36, 4),
+    ("REF_ROOM", 0, 64, 36, 4), ("REF_MATERIALS", 0, 64, 36, 4), ("TEXTURED", 0, 64, 36, 4),
 ])
 def test_sample_stream_render_matches_oracle(pt, kind, param, w, h, spp):
     """Production streams (one per pixel and sample): GPU vs the oracle's
@@ -184,7 +184,7 @@ def test_denoise_matches_oracle(pt):
 
 @pytest.mark.parametrize("kind,param,w,h,spp,aux", [
     ("ROOM_MESH", 6, 96, 64, 4, True), ("RANDOM_SPHERES", 0, 80, 45, 3, False), ("INSTANCES", 0, 64, 36, 2, True),
-    ("REF_MATERIALS", 0, 50, 30, 5, True),
+    ("REF_MATERIALS", 0, 50, 30, 5, True), ("TEXTURED", 0, 64, 36, 3, True),
 ])
 def test_wavefront_equals_megakernel(pt, kind, param, w, h, spp, aux):
     """The wavefront stages run the same per-slot arithmetic in the same order

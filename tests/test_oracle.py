@@ -53,7 +53,8 @@ def test_oracle_matches_reference_live(built):
         pytest.skip("reference harness absent")
     from photon_tracer_b200 import abi
     for kind, param, seed in [(abi.PT_GEN_ROOM_MESH, 3, 11), (abi.PT_GEN_REF_MATERIALS, 0, 1),
-                              (abi.PT_GEN_INSTANCES, 150, 4), (abi.PT_GEN_BATCH_SCENE, 0, 23)]:
+                              (abi.PT_GEN_INSTANCES, 150, 4), (abi.PT_GEN_BATCH_SCENE, 0, 23),
+                              (abi.PT_GEN_TEXTURED, 0, 7)]:
         g = built.Generated(kind, seed=seed, param=param)
         o, r = Oracle(g.desc), Reference(g.desc)
         rays = built.generate_rays(seed, [-4, -1, -4], [4, 3, 4], 5000)

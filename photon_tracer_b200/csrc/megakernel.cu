@@ -19,10 +19,12 @@ namespace {
 
 constexpr int kTileW = 8, kTileH = 4;
 
-// Resident 128-thread blocks per SM the register allocation targets (3:
-// at most 168 registers; measured best of 1..6 on the 1024x1024 room frame).
+// Resident 128-thread blocks per SM the register allocation targets (5: at
+// most 96 registers; with the flat-scene form's 58 bytes of spills, +6.6% on
+// the 1024x1024 room frame and +8% on the 10,000-instance frame against 3 and
+// 4, which the compiler met with 116-128 registers; 6 lost).
 #ifndef PT_MEGA_MIN_BLOCKS
-#define PT_MEGA_MIN_BLOCKS 3
+#define PT_MEGA_MIN_BLOCKS 5
 #endif
 
 template <bool AUX, bool SNAP, int TREES, bool TEX>
@@ -206,22 +208,27 @@ int occupancy(int threads, bool aux, bool snap) {
 // The single-loop traversal for scenes with instances, one loop per tree
 // otherwise; texture code only in the kernels for scenes with textures.
 bool one_loop(const PtSceneDev& S) { return S.use_bvh && S.inst_root != PT_NONE; }
+bool flat_only(const PtSceneDev& S) { return S.inst_root == PT_NONE && S.n_instances == 0; }
 
 }  // namespace
 
 cudaError_t pt_launch_megakernel(const PtSceneDev& S, const PtRenderParams& p, const PtLaunchShape& shape,
                                  cudaStream_t stream) {
     if (S.has_textures)
-        return one_loop(S) ? launch_form<PT_TREES_ONE, true>(S, p, shape, stream)
-                           : launch_form<PT_TREES_EACH, true>(S, p, shape, stream);
-    return one_loop(S) ? launch_form<PT_TREES_ONE, false>(S, p, shape, stream)
-                       : launch_form<PT_TREES_EACH, false>(S, p, shape, stream);
+        return one_loop(S)   ? launch_form<PT_TREES_ONE, true>(S, p, shape, stream)
+               : flat_only(S) ? launch_form<PT_TREES_FLAT, true>(S, p, shape, stream)
+                              : launch_form<PT_TREES_EACH, true>(S, p, shape, stream);
+    return one_loop(S)   ? launch_form<PT_TREES_ONE, false>(S, p, shape, stream)
+           : flat_only(S) ? launch_form<PT_TREES_FLAT, false>(S, p, shape, stream)
+                          : launch_form<PT_TREES_EACH, false>(S, p, shape, stream);
 }
 
 int pt_megakernel_blocks_per_sm(const PtSceneDev& S, int threads, bool aux, bool snapshot) {
     if (S.has_textures)
-        return one_loop(S) ? occupancy<PT_TREES_ONE, true>(threads, aux, snapshot)
-                           : occupancy<PT_TREES_EACH, true>(threads, aux, snapshot);
-    return one_loop(S) ? occupancy<PT_TREES_ONE, false>(threads, aux, snapshot)
-                       : occupancy<PT_TREES_EACH, false>(threads, aux, snapshot);
+        return one_loop(S)   ? occupancy<PT_TREES_ONE, true>(threads, aux, snapshot)
+               : flat_only(S) ? occupancy<PT_TREES_FLAT, true>(threads, aux, snapshot)
+                              : occupancy<PT_TREES_EACH, true>(threads, aux, snapshot);
+    return one_loop(S)   ? occupancy<PT_TREES_ONE, false>(threads, aux, snapshot)
+           : flat_only(S) ? occupancy<PT_TREES_FLAT, false>(threads, aux, snapshot)
+                          : occupancy<PT_TREES_EACH, false>(threads, aux, snapshot);
 }

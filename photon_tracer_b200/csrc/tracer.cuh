@@ -518,7 +518,8 @@ __device__ __forceinline__ int walk(const PtSceneDev& S, V wo, V wd, float t_min
 // picked per scene (instances present -> walk). The megakernel is built in
 // the two single forms and the host launches the one for its scene, so a
 // flat scene's kernel carries no two-level code.
-enum { PT_TREES_AUTO = 0, PT_TREES_EACH = 1, PT_TREES_ONE = 2 };
+// PT_TREES_FLAT: scenes without instances; no instance-tree code at all.
+enum { PT_TREES_AUTO = 0, PT_TREES_EACH = 1, PT_TREES_ONE = 2, PT_TREES_FLAT = 3 };
 
 template <bool COUNT, int TREES = PT_TREES_AUTO>
 __device__ __forceinline__ bool closest(const PtSceneDev& S, V o, V d, float t_min, float& t_max, Hit& h,
@@ -604,6 +605,15 @@ __device__ __forceinline__ bool closest(const PtSceneDev& S, V o, V d, float t_m
         return true;
     };
 
+    if constexpr (TREES == PT_TREES_FLAT) {
+        if (S.use_bvh) {
+            if (S.flat_root != PT_NONE)
+                if (!traverse<COUNT>(S.nodes, S.flat_root, o, d, t_min, t_max, stack, 0, cnt, flat_leaf)) return false;
+        } else if (S.n_flat_slots) {
+            flat_leaf(0, S.n_flat_slots | PT_LEAF_HAS_SPHERE, 0);
+        }
+        return true;
+    }
     if (S.use_bvh) {
 #if PT_TRAV_UNIFIED
         if constexpr (TREES != PT_TREES_EACH)
@@ -684,6 +694,18 @@ __device__ __forceinline__ bool occluded(const PtSceneDev& S, V o, V d, float t_
         if (blocked) t_far = t_min;
         return true;
     };
+    if constexpr (TREES == PT_TREES_FLAT) {
+        if (S.use_bvh) {
+            if (S.flat_root != PT_NONE &&
+                !traverse<COUNT>(S.nodes, S.flat_root, o, d, t_min, t_far, stack, 0, cnt, flat_leaf)) {
+                *overflow = true;
+                return false;
+            }
+        } else if (S.n_flat_slots) {
+            flat_leaf(0, S.n_flat_slots | PT_LEAF_HAS_SPHERE, 0);
+        }
+        return blocked;
+    }
     if (S.use_bvh) {
 #if PT_TRAV_UNIFIED
         if constexpr (TREES != PT_TREES_EACH) {

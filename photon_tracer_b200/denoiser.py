@@ -210,11 +210,25 @@ def main(argv=None) -> int:
     p = sub.add_parser("time")
     p.add_argument("--width", type=int, default=1920)
     p.add_argument("--height", type=int, default=1080)
+    f = sub.add_parser("frames", help="denoise seeded random frames with the trained weights (a profiling driver)")
+    f.add_argument("--count", type=int, default=3)
+    f.add_argument("--width", type=int, default=1920)
+    f.add_argument("--height", type=int, default=1080)
     args = ap.parse_args(argv)
     import torch
     torch.cuda.init()
     if args.cmd == "time":
         print(json.dumps(time_forward(UNet(seed=1), args.width, args.height)))
+        return 0
+    if args.cmd == "frames":
+        net = trained()
+        g = torch.Generator(device="cuda").manual_seed(1)
+        color = torch.rand((args.height, args.width, 3), device="cuda", generator=g)
+        aux = torch.rand((args.height, args.width, 7), device="cuda", generator=g)
+        depth = torch.rand((args.height, args.width), device="cuda", generator=g)
+        for _ in range(args.count):
+            net.denoise(color, aux, depth)
+        net.sync()
         return 0
     t0 = time.perf_counter()
     data = make_training_set(args.frames, args.size, args.target_spp, default_frames=args.default_frames)

@@ -34,6 +34,10 @@ __device__ __forceinline__ unsigned long long global_ns() {
 #define PT_BATCH_MIN_BLOCKS128 4
 #endif
 
+#ifndef PT_BATCH_ONE_QUERY
+#define PT_BATCH_ONE_QUERY 1
+#endif
+
 template <int THREADS, int TREES, bool TEX>
 __global__ void __launch_bounds__(THREADS, PT_BATCH_MIN_BLOCKS128 * 128 / THREADS)
     batch_megakernel(PtSceneDev S0, PtBatchLaunch B) {
@@ -52,6 +56,11 @@ __global__ void __launch_bounds__(THREADS, PT_BATCH_MIN_BLOCKS128 * 128 / THREAD
     Sampler smp;
     Rng rng;
     PtSceneDev S = S0;
+    // Scenes without instances: one ray query per trip, the pending shadow
+    // rays in shared memory (as in the single-scene megakernel).
+    constexpr bool ONE_QUERY = PT_BATCH_ONE_QUERY && TREES == PT_TREES_FLAT;
+    __shared__ float pend[10][ONE_QUERY ? THREADS : 1];
+    bool shadow_pending = false, done_after_shadow = false;
 
     while (true) {
         const bool need = !has_pixel && !exhausted;
@@ -132,7 +141,14 @@ __global__ void __launch_bounds__(THREADS, PT_BATCH_MIN_BLOCKS128 * 128 / THREAD
             }
         }
 
-        if (in_path) {
+        if constexpr (ONE_QUERY) {
+            if (in_path && query_trip<false, TEX>(S, path, depth, smp, rng, first, pend, shadow_pending,
+                                                  done_after_shadow, stack, rays, overflow)) {
+                acc = acc + path.rad;
+                in_path = false;
+                ++s;
+            }
+        } else if (in_path) {
             ++rays;
             smp.set_bounce(path.bounce);
             float t = 1000.0f;

@@ -137,6 +137,66 @@ __device__ __forceinline__ int shade(const PtSceneDev& S, Path& p, bool hit, con
     return p.bounce >= depth ? STEP_DONE : STEP_CONTINUE;
 }
 
+// One loop trip of a persistent kernel that traces ONE query per trip for a
+// scene without instances: the path's next closest hit (then its shading),
+// or the shadow ray the previous trip's shading made, which is resolved
+// before the path continues. Nothing between making the shadow ray and
+// resolving it consumes random numbers or touches the path's sums, so the
+// results are those of the inline form. The pending shadow ray (origin,
+// direction, t_max, unblocked value) of each thread sits in shared memory,
+// column threadIdx.x of pend. Returns true when the path has ended.
+template <bool AUX, bool TEX, int N>
+__device__ __forceinline__ bool query_trip(const PtSceneDev& S, Path& path, int depth, Sampler& smp, Rng& rng,
+                                           First& first, float (&pend)[10][N], bool& shadow_pending,
+                                           bool& done_after_shadow, StackEntry* stack, unsigned long long& rays,
+                                           bool& overflow) {
+    const int t = threadIdx.x;
+    const bool any = shadow_pending;
+    V qo, qd;
+    float tq;
+    if (any) {
+        qo = mk(pend[0][t], pend[1][t], pend[2][t]);
+        qd = mk(pend[3][t], pend[4][t], pend[5][t]);
+        tq = pend[6][t];
+    } else {
+        ++rays;
+        smp.set_bounce(path.bounce);
+        qo = path.o;
+        qd = path.d;
+        tq = 1000.0f;
+    }
+    Hit h;
+    if (!query_flat(S, qo, qd, 0.001f, tq, any, h, stack)) {
+        overflow = true;
+        h.kind = PT_HIT_NONE;
+    }
+    if (any) {
+        if (h.kind == PT_HIT_NONE) path.rad = path.rad + mk(pend[7][t], pend[8][t], pend[9][t]);
+        shadow_pending = false;
+        return done_after_shadow;
+    }
+    const bool hit = h.kind != PT_HIT_NONE;
+    Rec rec;
+    if (hit) fill<TEX>(S, h, path.o, path.d, tq, rec);
+    bool nee;
+    Shadow sh;
+    const bool done = shade<AUX, TEX>(S, path, hit, rec, depth, smp, rng, first, nee, sh, rays) == STEP_DONE;
+    if (!nee) return done;
+    pend[0][t] = sh.o.x;
+    pend[1][t] = sh.o.y;
+    pend[2][t] = sh.o.z;
+    pend[3][t] = sh.d.x;
+    pend[4][t] = sh.d.y;
+    pend[5][t] = sh.d.z;
+    pend[6][t] = sh.t_max;
+    pend[7][t] = sh.value.x;
+    pend[8][t] = sh.value.y;
+    pend[9][t] = sh.value.z;
+    shadow_pending = true;
+    done_after_shadow = done;
+    return false;
+}
+
 // luminance (include/renderer.hpp:364)
 __device__ __forceinline__ float luminance(V c) { return 0.2126f * c.x + 0.7152f * c.y + 0.0722f * c.z; }
 

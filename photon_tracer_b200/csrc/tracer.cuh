@@ -745,6 +745,59 @@ __device__ __forceinline__ bool occluded(const PtSceneDev& S, V o, V d, float t_
     return blocked;
 }
 
+// closest (any = false) and occluded (any = true) for a scene without
+// instances, through ONE traversal: a kernel that issues both kinds of query
+// from one call site carries one copy of the node and leaf code, and lanes
+// on a shadow ray traverse alongside lanes on a path ray. The any-hit form
+// stops at the first blocker (h.kind set), the point where occluded stops
+// doing work; until then both forms run the same tests with the same t_max,
+// so each returns what closest / occluded return. False when the stack
+// would overflow.
+__device__ __forceinline__ bool query_flat(const PtSceneDev& S, V o, V d, float t_min, float& t_max, bool any,
+                                           Hit& h, StackEntry* stack) {
+    h.kind = PT_HIT_NONE;
+    h.index = 0;
+    h.inst = 0;
+    h.u = 0;
+    h.v = 0;
+    for (uint32_t i = 0; i < S.n_large; ++i)
+        if (sphere_hit_double(__ldg(S.large + i), o, d, t_min, t_max)) {
+            h.kind = PT_HIT_LARGE;
+            h.index = i;
+            if (any) return true;
+        }
+    // false stops the traversal: only after an any-hit blocker.
+    auto leaf = [&](uint32_t first, uint32_t count_word, int) -> bool {
+        const uint32_t count = count_word & PT_COUNT_MASK;
+        const bool spheres = (count_word & PT_LEAF_HAS_SPHERE) != 0;
+        for (uint32_t k = first; k < first + count; ++k) {
+            const float4* s = S.slots + 3 * size_t(k);
+            const float4 c = __ldg(s + 2);
+            bool hit;
+            if (spheres && (fbits(c.y) & PT_SLOT_SPHERE)) {
+                hit = sphere_hit(__ldg(s), o, d, t_min, t_max);
+                if (hit) h.kind = PT_HIT_SPHERE;
+            } else {
+                hit = tri_hit(__ldg(s), __ldg(s + 1), c, o, d, t_min, t_max, h.u, h.v);
+                if (hit) h.kind = PT_HIT_TRIANGLE;
+            }
+            if (hit) {
+                h.index = k;
+                if (any) return false;
+            }
+        }
+        return true;
+    };
+    Counts cnt;
+    if (S.use_bvh) {
+        if (S.flat_root != PT_NONE && !traverse<false>(S.nodes, S.flat_root, o, d, t_min, t_max, stack, 0, cnt, leaf))
+            return any && h.kind != PT_HIT_NONE;
+    } else if (S.n_flat_slots) {
+        leaf(0, S.n_flat_slots | PT_LEAF_HAS_SPHERE, 0);
+    }
+    return true;
+}
+
 // The original primitive number of a closest hit (for ray queries).
 __device__ __forceinline__ void resolve(const PtSceneDev& S, const Hit& h, uint32_t& index, uint32_t& sub) {
     index = h.index;

@@ -32,6 +32,7 @@ constexpr int kTileX = 16, kTileY = 8, kM = kTileX * kTileY;  // 128 pixels = 12
 constexpr int kKc = 32;                                        // input channels per K step (64 bytes)
 constexpr int kStagesTile = 4;  // pipeline stages of the shifted-box form
 constexpr int kThreads = 192;  // warp 0: TMA, warp 1: TMEM + MMA, warps 2-5: epilogue
+constexpr int kMaxN = 256;     // output channels: two accumulators of N columns in 512
 constexpr uint32_t kABytes = kM * kKc * 2;
 constexpr unsigned long long kWaitNs = 1000000000ull;
 // The halo form (Cout <= 64): an 8 x 16 pixel tile whose 10 x 18 halo box is
@@ -160,6 +161,18 @@ __device__ __forceinline__ void tmem_ld16(uint32_t addr, float (&v)[16]) {
     for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
 
+// The same load without the wait: several may be in flight before one
+// tmem_wait(), and their registers are read only after it.
+__device__ __forceinline__ void tmem_ld16_async(uint32_t addr, uint32_t (&r)[16]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+        "%15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+          "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(addr));
+}
+__device__ __forceinline__ void tmem_wait() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
 __device__ __forceinline__ void bar_arrive(uint32_t bar) {
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
 }
@@ -235,6 +248,10 @@ __global__ void __launch_bounds__(kThreads) conv_tc_kernel(const __grid_constant
                      : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
+    // The bias once per CTA (zeros without one), read by the epilogue as
+    // shared-memory broadcasts.
+    __shared__ float sbias[kMaxN];
+    for (int i = threadIdx.x; i < N; i += kThreads) sbias[i] = bias ? bias[i] : 0.0f;
     fence_before();
     __syncthreads();
     fence_after();
@@ -343,12 +360,21 @@ __global__ void __launch_bounds__(kThreads) conv_tc_kernel(const __grid_constant
             const int ylane = HALO ? 8 : 16;
             const bool pool_writer = valid && !(lane & (1 | ylane));
             const size_t ppix = (size_t(b) * (H >> 1) + (py >> 1)) * (W >> 1) + (px >> 1);
-            for (int c = 0; c < N; c += 16) {
+            const uint32_t acc_addr = tmem + (uint32_t(q * 32) << 16) + uint32_t(a * (tmem_cols / 2));
+            for (int c0 = 0; c0 < N; c0 += 32) {
+              // two 16-column loads in flight per wait
+              uint32_t r[2][16];
+              tmem_ld16_async(acc_addr + uint32_t(c0), r[0]);
+              if (c0 + 16 < N) tmem_ld16_async(acc_addr + uint32_t(c0 + 16), r[1]);
+              tmem_wait();
+#pragma unroll
+              for (int h = 0; h < 2; ++h) {
+                const int c = c0 + 16 * h;
+                if (c >= N) break;
                 float v[16];
-                tmem_ld16(tmem + (uint32_t(q * 32) << 16) + uint32_t(a * (tmem_cols / 2) + c), v);
 #pragma unroll
                 for (int j = 0; j < 16; ++j) {
-                    v[j] += bias ? bias[c + j] : 0.0f;
+                    v[j] = __uint_as_float(r[h][j]) + sbias[c + j];
                     if (relu) v[j] = fmaxf(v[j], 0.0f);
                 }
                 if (OUT_F32) {
@@ -399,6 +425,7 @@ __global__ void __launch_bounds__(kThreads) conv_tc_kernel(const __grid_constant
                         dst[1] = p1;
                     }
                 }
+              }
             }
             // This warp's reads of the accumulator are done: the MMA warp may reuse it.
             fence_before();
@@ -433,15 +460,21 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
 }
 
 // Pipeline stages and dynamic shared memory of the two forms.
-int conv_stages(bool halo, int N) { return halo ? (N <= 32 ? 3 : 2) : kStagesTile; }
+#ifndef PT_CONV_HALO_MAX_N
+#define PT_CONV_HALO_MAX_N 64
+#endif
+#ifndef PT_CONV_HALO_STAGES32
+#define PT_CONV_HALO_STAGES32 3
+#endif
+int conv_stages(bool halo, int N) { return halo ? (N <= 32 ? PT_CONV_HALO_STAGES32 : 2) : kStagesTile; }
+// The halo form's A descriptors (LBO = one 2,880-byte plane, SBO = one
+// 160-byte halo row) reach at most 15 * 160 + 7 * 16 + 2,880 + 16 bytes past
+// a start of at most 2 * 2,880 + (2 * 10 + 2) * 16: exactly the 11,520 bytes
+// of the stage's halo.
 size_t smem_bytes(bool halo, int N) {
     const int st = conv_stages(halo, N);
     const size_t a = halo ? kHaloStage : kABytes, b = (halo ? 9 : 1) * size_t(N) * kKc * 2;
-    const size_t need = 1024 + st * (a + b) + (2 * st + 4) * 8 + 8;
-    // The halo form reads its A operand through descriptors with 2,880-byte
-    // strides; the allocation keeps 96 KB beyond the first stage so that no
-    // descriptor reach can leave it.
-    return halo ? std::max<size_t>(need, 1024 + 98304 + 128) : need;
+    return 1024 + st * (a + b) + (2 * st + 4) * 8 + 8;
 }
 
 // CTAs that fit on all SMs at once: the kernel's resident blocks per SM
@@ -623,7 +656,7 @@ cudaError_t conv_fwd_tc(const ConvShape& s, const __nv_bfloat16* in, const __nv_
     // The halo form for Cout <= 64 (where re-reading the shifted box per tap
     // bounds the kernel), the shifted-box form otherwise or if the halo's
     // tensor map is refused.
-    bool halo = N <= 64;
+    bool halo = N <= PT_CONV_HALO_MAX_N;
     CUtensorMap tm_in, tm_w;
     if (halo) {
         // [B][H][W][Cin] seen as (8 channels, x, y, channel group, image): the

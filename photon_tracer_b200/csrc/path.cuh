@@ -50,7 +50,9 @@ __device__ __forceinline__ bool direct_light_ray(const PtSceneDev& S, const Rec&
     const float cos_t = 1 - s1 * one_minus_cos_max;
     const float sin_t = sqrtf(fmaxf(0.0f, 1 - cos_t * cos_t));
     const float phi = 2 * float(M_PI) * s2;
-    const V dir = u * (cosf(phi) * sin_t) + v * (sinf(phi) * sin_t) + w * cos_t;
+    float sp, cp;
+    sin_cos(phi, sp, cp);
+    const V dir = u * (cp * sin_t) + v * (sp * sin_t) + w * cos_t;
     const float cos_surface = dot(dir, rec.normal);
     if (cos_surface <= 0) return false;
     float t_light = __int_as_float(0x7f800000);

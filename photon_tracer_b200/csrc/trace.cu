@@ -15,6 +15,9 @@ __device__ __forceinline__ void load_ray(const float* rays, size_t i, V& o, V& d
     d = mk(r[3], r[4], r[5]);
 }
 
+// FLAT: scenes without instances take the one-traversal query (no
+// instance-tree code in the kernel).
+template <bool FLAT>
 __global__ void __launch_bounds__(128) trace_closest_kernel(PtSceneDev S, const float* __restrict__ rays, size_t n,
                                                              float tmin, float tmax, pt_hit* __restrict__ hits) {
     StackEntry stack[PT_STACK_MAX];
@@ -24,8 +27,14 @@ __global__ void __launch_bounds__(128) trace_closest_kernel(PtSceneDev S, const 
         load_ray(rays, i, o, d);
         float t = tmax;
         Hit h;
-        Counts cnt;
-        if (!closest<false>(S, o, d, tmin, t, h, stack, cnt)) {
+        bool ok;
+        if constexpr (FLAT) {
+            ok = query_flat(S, o, d, tmin, t, false, h, stack);
+        } else {
+            Counts cnt;
+            ok = closest<false>(S, o, d, tmin, t, h, stack, cnt);
+        }
+        if (!ok) {
             overflow = true;
             h.kind = PT_HIT_NONE;
         }
@@ -43,6 +52,7 @@ __global__ void __launch_bounds__(128) trace_closest_kernel(PtSceneDev S, const 
     if (overflow) atomicOr(S.status, PT_DEV_ERR_STACK);
 }
 
+template <bool FLAT>
 __global__ void __launch_bounds__(128) trace_any_kernel(PtSceneDev S, const float* __restrict__ rays, size_t n,
                                                          float tmin, float tmax, uint8_t* __restrict__ occ) {
     StackEntry stack[PT_STACK_MAX];
@@ -50,10 +60,19 @@ __global__ void __launch_bounds__(128) trace_any_kernel(PtSceneDev S, const floa
     for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x) {
         V o, d;
         load_ray(rays, i, o, d);
-        Counts cnt;
-        bool ovf = false;
-        const bool b = occluded<false>(S, o, d, tmin, tmax, stack, cnt, &ovf);
-        overflow |= ovf;
+        bool b;
+        if constexpr (FLAT) {
+            float t = tmax;
+            Hit h;
+            const bool ok = query_flat(S, o, d, tmin, t, true, h, stack);
+            overflow |= !ok;
+            b = ok && h.kind != PT_HIT_NONE;
+        } else {
+            Counts cnt;
+            bool ovf = false;
+            b = occluded<false>(S, o, d, tmin, tmax, stack, cnt, &ovf);
+            overflow |= ovf;
+        }
         occ[i] = b ? 1 : 0;
     }
     if (overflow) atomicOr(S.status, PT_DEV_ERR_STACK);
@@ -110,6 +129,8 @@ __global__ void __launch_bounds__(128) primary_depth_kernel(PtSceneDev S, PtCamD
     if (overflow) atomicOr(S.status, PT_DEV_ERR_STACK);
 }
 
+bool flat_scene(const PtSceneDev& S) { return S.inst_root == PT_NONE && S.n_instances == 0; }
+
 int grid_for(size_t n, int threads) {
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
@@ -124,14 +145,20 @@ int grid_for(size_t n, int threads) {
 cudaError_t pt_launch_trace_closest(const PtSceneDev& S, const float* rays, size_t n, float tmin, float tmax,
                                     void* hits, cudaStream_t stream) {
     if (n == 0) return cudaSuccess;
-    trace_closest_kernel<<<grid_for(n, 128), 128, 0, stream>>>(S, rays, n, tmin, tmax, static_cast<pt_hit*>(hits));
+    if (flat_scene(S))
+        trace_closest_kernel<true><<<grid_for(n, 128), 128, 0, stream>>>(S, rays, n, tmin, tmax, static_cast<pt_hit*>(hits));
+    else
+        trace_closest_kernel<false><<<grid_for(n, 128), 128, 0, stream>>>(S, rays, n, tmin, tmax, static_cast<pt_hit*>(hits));
     return cudaGetLastError();
 }
 
 cudaError_t pt_launch_trace_any(const PtSceneDev& S, const float* rays, size_t n, float tmin, float tmax,
                                 uint8_t* occ, cudaStream_t stream) {
     if (n == 0) return cudaSuccess;
-    trace_any_kernel<<<grid_for(n, 128), 128, 0, stream>>>(S, rays, n, tmin, tmax, occ);
+    if (flat_scene(S))
+        trace_any_kernel<true><<<grid_for(n, 128), 128, 0, stream>>>(S, rays, n, tmin, tmax, occ);
+    else
+        trace_any_kernel<false><<<grid_for(n, 128), 128, 0, stream>>>(S, rays, n, tmin, tmax, occ);
     return cudaGetLastError();
 }
 

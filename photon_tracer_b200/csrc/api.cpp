@@ -260,6 +260,7 @@ pt_status pt_scene_create(const pt_scene_desc* desc, pt_scene** out) {
     D.tex = upload(base, off, A.tex, err);
     D.texels = upload(base, off, A.texels, err);
     D.has_textures = A.has_textures;
+    D.ordered_boxes = ordered_boxes(A.nodes);
     s->status = reinterpret_cast<unsigned int*>(base + off);
     off += 256;
     s->work = reinterpret_cast<unsigned int*>(base + off);

@@ -397,6 +397,7 @@ pt_status pt_batch_create(const pt_batch_item* items, uint32_t n, int32_t strate
     D.tex = upload(base, off, all.tex, err);
     D.texels = upload(base, off, all.texels, err);
     D.has_textures = all.has_textures;
+    D.ordered_boxes = ordered_boxes(all.nodes);
     b->d_scenes = upload(base, off, b->scenes, err);
     b->d_out = reinterpret_cast<float*>(base + off);
     off += align256(out_floats * 4);

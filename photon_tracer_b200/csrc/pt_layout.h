@@ -102,4 +102,5 @@ struct PtSceneDev {
     uint32_t n_spheres;       // top-level spheres
     int sky, sample_lights, use_bvh;
     int has_textures;         // some lambertian has a texture
+    int ordered_boxes;        // every node child box has lo <= hi on each axis (no NaN)
 };

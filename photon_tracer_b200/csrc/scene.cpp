@@ -353,4 +353,11 @@ pt_status build_arena(const pt_scene_desc& d, HostArena& A) {
     return PT_OK;
 }
 
+int ordered_boxes(const std::vector<float>& nodes) {
+    for (size_t k = 0; k + 32 <= nodes.size(); k += 32)
+        for (int i = 0; i < 12; ++i)
+            if (!(nodes[k + i] <= nodes[k + 12 + i])) return 0;
+    return 1;
+}
+
 }  // namespace pt

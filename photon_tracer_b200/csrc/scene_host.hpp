@@ -34,4 +34,9 @@ struct HostArena {
 
 pt_status build_arena(const pt_scene_desc& d, HostArena& A);
 
+// 1 when every child box of every node (32 floats per node: lo[3][4],
+// hi[3][4], first[4], count[4]) has lo <= hi on each axis, i.e. holds no NaN
+// and is not inverted; the traversal's fast slab test relies on it.
+int ordered_boxes(const std::vector<float>& nodes);
+
 }  // namespace pt

@@ -167,7 +167,14 @@ __device__ __forceinline__ V aff_transposed(const float4 r[3], V v) {
 //    a finite origin, while t_max is not NaN, no operand is NaN and the two
 //    forms agree (a -0/+0 difference cannot change any comparison the
 //    traversal makes), so those nodes use the one-instruction min/max; other
-//    rays keep the exact emulation.
+//    rays keep the exact emulation. The node boxes must be NaN-free too
+//    (PtSceneDev::ordered_boxes: lo <= hi for every child and axis, which
+//    the empty-child encoding lo = hi = +inf also meets). Then, with the
+//    sign of each inverse direction known, (lo - o) * inv <= (hi - o) * inv
+//    or the reverse holds for every child (rounding is monotonic), so the
+//    per-axis min / max is the value from the near plane / far plane: fast
+//    rays load the near planes where the emulation reads lo and skip the
+//    six per-axis min / max of each child.
 //  * PT_TRAV_F32X2: the six subtractions and six multiplications of two
 //    children's slabs are issued as packed pairs (sub/mul.rn.f32x2), which
 //    round each lane exactly as the scalar instructions do.
@@ -220,11 +227,15 @@ __device__ __forceinline__ void child_ranks(const float (&tn)[4], int mask, int 
 }
 
 template <bool COUNT, class Leaf>
-__device__ __forceinline__ bool traverse(const float4* __restrict__ nodes, uint32_t root, V o, V d, float t_min,
-                                         float& t_max, StackEntry* stack, int base, Counts& cnt, Leaf&& leaf) {
+__device__ __forceinline__ bool traverse(const PtSceneDev& S, uint32_t root, V o, V d, float t_min, float& t_max,
+                                         StackEntry* stack, int base, Counts& cnt, Leaf&& leaf) {
+    const float4* __restrict__ nodes = S.nodes;
     const float ix = 1.0f / d.x, iy = 1.0f / d.y, iz = 1.0f / d.z;
-    const bool ray_fast = PT_TRAV_FAST_MINMAX && finite_nonzero(ix) && finite_nonzero(iy) && finite_nonzero(iz) &&
-                          finite_f(o.x) && finite_f(o.y) && finite_f(o.z) && t_min == t_min;
+    const bool ray_fast = PT_TRAV_FAST_MINMAX && S.ordered_boxes && finite_nonzero(ix) && finite_nonzero(iy) &&
+                          finite_nonzero(iz) && finite_f(o.x) && finite_f(o.y) && finite_f(o.z) && t_min == t_min;
+    // float4 index of each axis' near plane (lo: 0-2, hi: 3-5); the far
+    // plane is the other one.
+    const int nx = ray_fast && ix < 0 ? 3 : 0, ny = ray_fast && iy < 0 ? 4 : 1, nz = ray_fast && iz < 0 ? 5 : 2;
     int top = base;
     uint32_t cf = root, cc = 0;
     float ct = t_min;
@@ -248,12 +259,13 @@ __device__ __forceinline__ bool traverse(const float4* __restrict__ nodes, uint3
             continue;
         }
         const float4* nd = nodes + 8 * size_t(cf);
-        const float4 lox = __ldg(nd + 0), loy = __ldg(nd + 1), loz = __ldg(nd + 2);
-        const float4 hix = __ldg(nd + 3), hiy = __ldg(nd + 4), hiz = __ldg(nd + 5);
+        const float4 lox = __ldg(nd + nx), loy = __ldg(nd + ny), loz = __ldg(nd + nz);
+        const float4 hix = __ldg(nd + (3 - nx)), hiy = __ldg(nd + (5 - ny)), hiz = __ldg(nd + (7 - nz));
         const uint4 first = __ldg(reinterpret_cast<const uint4*>(nd + 6));
         const uint4 count = __ldg(reinterpret_cast<const uint4*>(nd + 7));
         if (COUNT) cnt.nodes++;
-        // Slab values per child: x0 = (lo.x - o.x) * ix ... z1 = (hi.z - o.z) * iz.
+        // Slab values per child: x0 = (lo.x - o.x) * ix ... z1 = (hi.z - o.z) * iz
+        // (for fast rays lo / hi are the near / far planes).
         float X0[4], X1[4], Y0[4], Y1[4], Z0[4], Z1[4];
         if (PT_TRAV_F32X2) {
             const float2 ox = make_float2(o.x, o.x), oy = make_float2(o.y, o.y), oz = make_float2(o.z, o.z);
@@ -288,10 +300,12 @@ __device__ __forceinline__ bool traverse(const float4* __restrict__ nodes, uint3
         float tn[4];
         int mask = 0;
         if (ray_fast && t_max == t_max) {
+            // near plane values are each axis' minimum (lo <= hi, sign of
+            // the inverse direction known): no per-axis min / max
 #pragma unroll
             for (int c = 0; c < 4; ++c) {
-                const float n_ = fmaxf(fmaxf(fminf(X0[c], X1[c]), fminf(Y0[c], Y1[c])), fmaxf(fminf(Z0[c], Z1[c]), t_min));
-                const float f_ = fminf(fminf(fmaxf(X0[c], X1[c]), fmaxf(Y0[c], Y1[c])), fminf(fmaxf(Z0[c], Z1[c]), t_max));
+                const float n_ = fmaxf(fmaxf(X0[c], Y0[c]), fmaxf(Z0[c], t_min));
+                const float f_ = fminf(fminf(X1[c], Y1[c]), fminf(Z1[c], t_max));
                 tn[c] = n_;
                 mask |= (n_ <= f_) ? (1 << c) : 0;
             }
@@ -359,14 +373,18 @@ struct TravRay {
     V o, d;
     float ix, iy, iz;
     bool fast;
-    __device__ __forceinline__ void set(V o_, V d_, float t_min) {
+    int nx, ny, nz;  // float4 index of each axis' near plane (lo: 0-2, hi: 3-5)
+    __device__ __forceinline__ void set(V o_, V d_, float t_min, bool ordered) {
         o = o_;
         d = d_;
         ix = 1.0f / d.x;
         iy = 1.0f / d.y;
         iz = 1.0f / d.z;
-        fast = PT_TRAV_FAST_MINMAX && finite_nonzero(ix) && finite_nonzero(iy) && finite_nonzero(iz) &&
+        fast = PT_TRAV_FAST_MINMAX && ordered && finite_nonzero(ix) && finite_nonzero(iy) && finite_nonzero(iz) &&
                finite_f(o.x) && finite_f(o.y) && finite_f(o.z) && t_min == t_min;
+        nx = fast && ix < 0 ? 3 : 0;
+        ny = fast && iy < 0 ? 4 : 1;
+        nz = fast && iz < 0 ? 5 : 2;
     }
 };
 
@@ -376,8 +394,8 @@ template <bool COUNT>
 __device__ __forceinline__ bool expand_node(const float4* __restrict__ nodes, uint32_t cf, const TravRay& r,
                                             float t_min, float t_max, StackEntry* stack, int& top, Counts& cnt) {
     const float4* nd = nodes + 8 * size_t(cf);
-    const float4 lox = __ldg(nd + 0), loy = __ldg(nd + 1), loz = __ldg(nd + 2);
-    const float4 hix = __ldg(nd + 3), hiy = __ldg(nd + 4), hiz = __ldg(nd + 5);
+    const float4 lox = __ldg(nd + r.nx), loy = __ldg(nd + r.ny), loz = __ldg(nd + r.nz);
+    const float4 hix = __ldg(nd + (3 - r.nx)), hiy = __ldg(nd + (5 - r.ny)), hiz = __ldg(nd + (7 - r.nz));
     const uint4 first = __ldg(reinterpret_cast<const uint4*>(nd + 6));
     const uint4 count = __ldg(reinterpret_cast<const uint4*>(nd + 7));
     if (COUNT) cnt.nodes++;
@@ -404,8 +422,8 @@ __device__ __forceinline__ bool expand_node(const float4* __restrict__ nodes, ui
     if (r.fast && t_max == t_max) {
 #pragma unroll
         for (int c = 0; c < 4; ++c) {
-            const float n_ = fmaxf(fmaxf(fminf(X0[c], X1[c]), fminf(Y0[c], Y1[c])), fmaxf(fminf(Z0[c], Z1[c]), t_min));
-            const float f_ = fminf(fminf(fmaxf(X0[c], X1[c]), fmaxf(Y0[c], Y1[c])), fminf(fmaxf(Z0[c], Z1[c]), t_max));
+            const float n_ = fmaxf(fmaxf(X0[c], Y0[c]), fmaxf(Z0[c], t_min));
+            const float f_ = fminf(fminf(X1[c], Y1[c]), fminf(Z1[c], t_max));
             tn[c] = n_;
             mask |= (n_ <= f_) ? (1 << c) : 0;
         }
@@ -443,7 +461,7 @@ template <bool COUNT, bool ANY>
 __device__ __forceinline__ int walk(const PtSceneDev& S, V wo, V wd, float t_min, float& t_max, Hit& h,
                                     StackEntry* stack, Counts& cnt) {
     TravRay r;
-    r.set(wo, wd, t_min);
+    r.set(wo, wd, t_min, S.ordered_boxes);
     uint32_t cur_inst = 0;
     bool in_mesh = false;
     int top = 0;
@@ -453,7 +471,7 @@ __device__ __forceinline__ int walk(const PtSceneDev& S, V wo, V wd, float t_min
         const StackEntry e = stack[--top];
         uint32_t k = e.first, end = 0;
         if (e.pad == PT_ENT_WORLD) {
-            r.set(wo, wd, t_min);
+            r.set(wo, wd, t_min, S.ordered_boxes);
             in_mesh = false;
             continue;
         }
@@ -520,7 +538,7 @@ __device__ __forceinline__ int walk(const PtSceneDev& S, V wo, V wd, float t_min
         if (k + 1 < end) stack[top++] = {k + 1, end, -__int_as_float(0x7f800000), PT_ENT_RESUME};
         stack[top++] = {0u, 0u, -__int_as_float(0x7f800000), PT_ENT_WORLD};
         stack[top++] = {meta.x, 0u, t_min, PT_ENT_NODE};
-        r.set(aff_point(rows, wo), aff_vector(rows, wd), t_min);
+        r.set(aff_point(rows, wo), aff_vector(rows, wd), t_min, S.ordered_boxes);
         cur_inst = meta.y;
         in_mesh = true;
     }
@@ -613,7 +631,7 @@ __device__ __forceinline__ bool closest(const PtSceneDev& S, V o, V d, float t_m
                 }
                 return true;
             };
-            if (!traverse<COUNT>(S.nodes, meta.x, lo, ld, t_min, t_max, stack, top, cnt, mesh_leaf)) return false;
+            if (!traverse<COUNT>(S, meta.x, lo, ld, t_min, t_max, stack, top, cnt, mesh_leaf)) return false;
             if (found) {
                 h.kind = PT_HIT_INSTANCE;
                 h.index = slot;
@@ -628,7 +646,7 @@ __device__ __forceinline__ bool closest(const PtSceneDev& S, V o, V d, float t_m
     if constexpr (TREES == PT_TREES_FLAT) {
         if (S.use_bvh) {
             if (S.flat_root != PT_NONE)
-                if (!traverse<COUNT>(S.nodes, S.flat_root, o, d, t_min, t_max, stack, 0, cnt, flat_leaf)) return false;
+                if (!traverse<COUNT>(S, S.flat_root, o, d, t_min, t_max, stack, 0, cnt, flat_leaf)) return false;
         } else if (S.n_flat_slots) {
             flat_leaf(0, S.n_flat_slots | PT_LEAF_HAS_SPHERE, 0);
         }
@@ -641,9 +659,9 @@ __device__ __forceinline__ bool closest(const PtSceneDev& S, V o, V d, float t_m
                 return !(walk<COUNT, false>(S, o, d, t_min, t_max, h, stack, cnt) & 1);
 #endif
         if (S.flat_root != PT_NONE)
-            if (!traverse<COUNT>(S.nodes, S.flat_root, o, d, t_min, t_max, stack, 0, cnt, flat_leaf)) return false;
+            if (!traverse<COUNT>(S, S.flat_root, o, d, t_min, t_max, stack, 0, cnt, flat_leaf)) return false;
         if (S.inst_root != PT_NONE)
-            if (!traverse<COUNT>(S.nodes, S.inst_root, o, d, t_min, t_max, stack, 0, cnt, inst_leaf)) return false;
+            if (!traverse<COUNT>(S, S.inst_root, o, d, t_min, t_max, stack, 0, cnt, inst_leaf)) return false;
     } else {
         // Without the BVH every primitive, then every instance, in order (:135-139).
         if (S.n_flat_slots) flat_leaf(0, S.n_flat_slots | PT_LEAF_HAS_SPHERE, 0);
@@ -708,7 +726,7 @@ __device__ __forceinline__ bool occluded(const PtSceneDev& S, V o, V d, float t_
                 }
                 return true;
             };
-            if (!traverse<COUNT>(S.nodes, meta.x, lo, ld, t_min, t_mesh, stack, top, cnt, mesh_leaf)) return false;
+            if (!traverse<COUNT>(S, meta.x, lo, ld, t_min, t_mesh, stack, top, cnt, mesh_leaf)) return false;
             blocked = found;
         }
         if (blocked) t_far = t_min;
@@ -717,7 +735,7 @@ __device__ __forceinline__ bool occluded(const PtSceneDev& S, V o, V d, float t_
     if constexpr (TREES == PT_TREES_FLAT) {
         if (S.use_bvh) {
             if (S.flat_root != PT_NONE &&
-                !traverse<COUNT>(S.nodes, S.flat_root, o, d, t_min, t_far, stack, 0, cnt, flat_leaf)) {
+                !traverse<COUNT>(S, S.flat_root, o, d, t_min, t_far, stack, 0, cnt, flat_leaf)) {
                 *overflow = true;
                 return false;
             }
@@ -741,13 +759,13 @@ __device__ __forceinline__ bool occluded(const PtSceneDev& S, V o, V d, float t_
         }
 #endif
         if (S.flat_root != PT_NONE)
-            if (!traverse<COUNT>(S.nodes, S.flat_root, o, d, t_min, t_far, stack, 0, cnt, flat_leaf)) {
+            if (!traverse<COUNT>(S, S.flat_root, o, d, t_min, t_far, stack, 0, cnt, flat_leaf)) {
                 *overflow = true;
                 return false;
             }
         if (!blocked && S.inst_root != PT_NONE) {
             t_far = t_max;
-            if (!traverse<COUNT>(S.nodes, S.inst_root, o, d, t_min, t_far, stack, 0, cnt, inst_leaf)) {
+            if (!traverse<COUNT>(S, S.inst_root, o, d, t_min, t_far, stack, 0, cnt, inst_leaf)) {
                 *overflow = true;
                 return false;
             }
@@ -810,7 +828,7 @@ __device__ __forceinline__ bool query_flat(const PtSceneDev& S, V o, V d, float 
     };
     Counts cnt;
     if (S.use_bvh) {
-        if (S.flat_root != PT_NONE && !traverse<false>(S.nodes, S.flat_root, o, d, t_min, t_max, stack, 0, cnt, leaf))
+        if (S.flat_root != PT_NONE && !traverse<false>(S, S.flat_root, o, d, t_min, t_max, stack, 0, cnt, leaf))
             return any && h.kind != PT_HIT_NONE;
     } else if (S.n_flat_slots) {
         leaf(0, S.n_flat_slots | PT_LEAF_HAS_SPHERE, 0);

@@ -206,20 +206,26 @@ template <bool OUT_F32, bool HALO>
 __global__ void __launch_bounds__(kThreads) conv_tc_kernel(const __grid_constant__ CUtensorMap tm_in,
                                                            const __grid_constant__ CUtensorMap tm_w, int B, int H,
                                                            int W, int Cin, int N, int tmem_cols, int stages,
-                                                           const float* __restrict__ bias, int relu,
+                                                           int res, const float* __restrict__ bias, int relu,
                                                            const unet::ConvOut o, unsigned int* __restrict__ status) {
     extern __shared__ uint8_t smem_raw[];
     uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    const int chunks = Cin / kKc, iters = HALO ? chunks : 9 * chunks;
     const uint32_t tap_bytes = uint32_t(N) * kKc * 2;  // one tap's weights for 32 channels
-    const uint32_t a_bytes = HALO ? kHaloStage : kABytes, b_bytes = HALO ? 9 * tap_bytes : tap_bytes;
-    uint8_t* sa = smem;
-    uint8_t* sb = smem + stages * a_bytes;
-    // full[S], empty[S], acc_full[2], acc_empty[2]
+    // res (halo form only): all 9 x chunks weight boxes stay in shared memory
+    // for the CTA's life, loaded once; the stages carry only the halo.
+    const uint32_t w_bytes = res ? 9u * uint32_t(chunks) * tap_bytes : 0u;
+    const uint32_t a_bytes = HALO ? kHaloStage : kABytes, b_bytes = res ? 0u : (HALO ? 9 * tap_bytes : tap_bytes);
+    uint8_t* sw = smem;
+    uint8_t* sa = smem + w_bytes;
+    uint8_t* sb = sa + stages * a_bytes;
+    // full[S], empty[S], acc_full[2], acc_empty[2], weights
     uint64_t* bars = reinterpret_cast<uint64_t*>(sb + stages * b_bytes);
-    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * stages + 4);
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * stages + 5);
     volatile int* abort = reinterpret_cast<volatile int*>(tmem_slot + 1);
     const uint32_t full0 = smem_u32(bars), empty0 = smem_u32(bars + stages);
     const uint32_t acc_full0 = smem_u32(bars + 2 * stages), acc_empty0 = smem_u32(bars + 2 * stages + 2);
+    const uint32_t wbar = smem_u32(bars + 2 * stages + 4);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     TileGrid grid;
@@ -228,7 +234,6 @@ __global__ void __launch_bounds__(kThreads) conv_tc_kernel(const __grid_constant
     grid.tiles_x = (W + grid.tx - 1) / grid.tx;
     grid.tiles_y = (H + grid.ty - 1) / grid.ty;
     grid.n = grid.tiles_x * grid.tiles_y * B;
-    const int chunks = Cin / kKc, iters = HALO ? chunks : 9 * chunks;
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < stages; ++s) {
@@ -239,6 +244,7 @@ __global__ void __launch_bounds__(kThreads) conv_tc_kernel(const __grid_constant
             bar_init(acc_full0 + 8 * a, 1);
             bar_init(acc_empty0 + 8 * a, 4);  // one arrival per epilogue warp
         }
+        bar_init(wbar, 1);
         *abort = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
@@ -262,6 +268,12 @@ __global__ void __launch_bounds__(kThreads) conv_tc_kernel(const __grid_constant
         if (lane == 0) {
             asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&tm_in)) : "memory");
             asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&tm_w)) : "memory");
+            if (res) {
+                bar_expect_tx(wbar, w_bytes);
+                for (int ch = 0; ch < chunks; ++ch)
+                    for (int tap = 0; tap < 9; ++tap)
+                        tma_load_3d(smem_u32(sw + (ch * 9 + tap) * tap_bytes), &tm_w, ch * kKc, tap, 0, wbar);
+            }
             int g = 0;  // k steps issued so far, over all of this CTA's tiles
             for (int t = blockIdx.x; t < grid.n && ok; t += gridDim.x) {
                 int x0, y0, b;
@@ -275,10 +287,12 @@ __global__ void __launch_bounds__(kThreads) conv_tc_kernel(const __grid_constant
                     if (HALO) {
                         // the halo box of 32 channels (4 planes), and the 9 taps' weights for them
                         const int c0 = it * kKc;
-                        bar_expect_tx(full0 + 8 * s, kHaloBytes + b_bytes);
+                        bar_expect_tx(full0 + 8 * s, kHaloBytes + 9 * (res ? 0u : tap_bytes));
                         tma_load_5d(smem_u32(sa + s * a_bytes), &tm_in, 0, x0 - 1, y0 - 1, c0 / 8, b, full0 + 8 * s);
-                        for (int tap = 0; tap < 9; ++tap)
-                            tma_load_3d(smem_u32(sb + s * b_bytes + tap * tap_bytes), &tm_w, c0, tap, 0, full0 + 8 * s);
+                        if (!res)
+                            for (int tap = 0; tap < 9; ++tap)
+                                tma_load_3d(smem_u32(sb + s * b_bytes + tap * tap_bytes), &tm_w, c0, tap, 0,
+                                            full0 + 8 * s);
                     } else {
                         const int tap = it / chunks, c0 = (it - tap * chunks) * kKc;
                         bar_expect_tx(full0 + 8 * s, kABytes + b_bytes);
@@ -291,6 +305,7 @@ __global__ void __launch_bounds__(kThreads) conv_tc_kernel(const __grid_constant
             // The copies issued into each stage have landed before the CTA can exit.
             for (int k = g > stages ? g - stages : 0; k < g; ++k)
                 if (!wait_bar(full0 + 8 * (k % stages), (k / stages) & 1, nullptr)) ok = false;
+            if (res && !wait_bar(wbar, 0, nullptr)) ok = false;
         }
     } else if (warp == 1) {
         if (lane == 0) {
@@ -299,6 +314,7 @@ __global__ void __launch_bounds__(kThreads) conv_tc_kernel(const __grid_constant
             // 17, M >> 4 at bit 24.
             const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | (uint32_t(N >> 3) << 17) | (uint32_t(kM >> 4) << 24);
             int g = 0, i = 0;
+            if (res && !wait_bar(wbar, 0, abort)) ok = false;
             for (int t = blockIdx.x; t < grid.n && ok; t += gridDim.x, ++i) {
                 const int a = i & 1;
                 if (i >= 2 && !wait_bar(acc_empty0 + 8 * a, ((i >> 1) - 1) & 1, abort)) {
@@ -317,7 +333,8 @@ __global__ void __launch_bounds__(kThreads) conv_tc_kernel(const __grid_constant
                     if (HALO) {
                         // tap (dy, dx) reads the halo from offset (dy + 1, dx + 1): 8-pixel
                         // rows 10 pixels apart (SBO 160 B), K planes 2,880 B apart (LBO)
-                        const uint32_t a0 = smem_u32(sa + s * a_bytes), b0 = smem_u32(sb + s * b_bytes);
+                        const uint32_t a0 = smem_u32(sa + s * a_bytes);
+                        const uint32_t b0 = res ? smem_u32(sw + it * 9 * tap_bytes) : smem_u32(sb + s * b_bytes);
                         for (int tap = 0; tap < 9; ++tap) {
                             const uint32_t off = uint32_t((tap / 3) * kHaloW + tap % 3) * 16u;
                             const uint64_t bd = sw64_desc(b0 + tap * tap_bytes);
@@ -463,18 +480,43 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
 #ifndef PT_CONV_HALO_MAX_N
 #define PT_CONV_HALO_MAX_N 64
 #endif
-#ifndef PT_CONV_HALO_STAGES32
-#define PT_CONV_HALO_STAGES32 3
-#endif
-int conv_stages(bool halo, int N) { return halo ? (N <= 32 ? PT_CONV_HALO_STAGES32 : 2) : kStagesTile; }
 // The halo form's A descriptors (LBO = one 2,880-byte plane, SBO = one
 // 160-byte halo row) reach at most 15 * 160 + 7 * 16 + 2,880 + 16 bytes past
 // a start of at most 2 * 2,880 + (2 * 10 + 2) * 16: exactly the 11,520 bytes
 // of the stage's halo.
-size_t smem_bytes(bool halo, int N) {
-    const int st = conv_stages(halo, N);
-    const size_t a = halo ? kHaloStage : kABytes, b = (halo ? 9 : 1) * size_t(N) * kKc * 2;
-    return 1024 + st * (a + b) + (2 * st + 4) * 8 + 8;
+size_t conv_smem(bool halo, bool res, int Cin, int N, int stages) {
+    const size_t tap = size_t(N) * kKc * 2;
+    const size_t w = res ? 9 * tap * size_t(Cin / kKc) : 0;
+    const size_t a = halo ? kHaloStage : kABytes, b = res ? 0 : (halo ? 9 : 1) * tap;
+    return 1024 + w + stages * (a + b) + (2 * stages + 5) * 8 + 8;
+}
+
+// Shared memory layout of one launch. The halo form keeps its weights
+// resident when they take at most 80 KB, with as many halo stages (2 to 6)
+// as leave three CTAs per SM, else two (228 KB per SM, 1 KB reserved and
+// 1 KB of bias per CTA); bigger weights stream with each stage.
+struct ConvPlan {
+    bool halo, res;
+    int stages;
+    size_t smem;
+};
+constexpr size_t kSmemPerSM = 228 * 1024, kResMaxBytes = 80 * 1024;
+#ifndef PT_CONV_RESIDENT
+#define PT_CONV_RESIDENT 1
+#endif
+ConvPlan conv_plan(bool halo, int Cin, int N) {
+    ConvPlan p{halo, false, halo ? (N <= 32 ? 3 : 2) : kStagesTile, 0};
+    if (PT_CONV_RESIDENT && halo && size_t(9) * Cin * N * 2 <= kResMaxBytes) {
+        for (int ctas = 3; ctas >= 2 && !p.res; --ctas)
+            for (int st = 6; st >= 2; --st)
+                if (conv_smem(true, true, Cin, N, st) <= kSmemPerSM / ctas - 2048) {
+                    p.res = true;
+                    p.stages = st;
+                    break;
+                }
+    }
+    p.smem = conv_smem(halo, p.res, Cin, N, p.stages);
+    return p;
 }
 
 // CTAs that fit on all SMs at once: the kernel's resident blocks per SM
@@ -693,8 +735,9 @@ cudaError_t conv_fwd_tc(const ConvShape& s, const __nv_bfloat16* in, const __nv_
     }
     int cols = 32;
     while (cols < 2 * N) cols *= 2;  // two accumulators
-    const size_t smem = smem_bytes(halo, N);
-    const int stages = conv_stages(halo, N);
+    const ConvPlan plan = conv_plan(halo, s.Cin, N);
+    const size_t smem = plan.smem;
+    const int stages = plan.stages;
     const int tx = halo ? kHaloTX : kTileX, ty = halo ? kHaloTY : kTileY;
     const long tiles = long((s.W + tx - 1) / tx) * ((s.H + ty - 1) / ty) * s.B;
     if (tiles > 0x7fffffffL) return cudaErrorNotSupported;
@@ -707,8 +750,8 @@ cudaError_t conv_fwd_tc(const ConvShape& s, const __nv_bfloat16* in, const __nv_
     const long g = grid_size(cols, smem, fn);
     const unsigned blocks = unsigned(tiles < g ? tiles : g);
 #define PT_CONV_LAUNCH(F32, HALO)                                                                                     \
-    conv_tc_kernel<F32, HALO><<<blocks, kThreads, smem, st>>>(tm_in, tm_w, s.B, s.H, s.W, s.Cin, N, cols, stages, bias, \
-                                                             relu, o, status)
+    conv_tc_kernel<F32, HALO><<<blocks, kThreads, smem, st>>>(tm_in, tm_w, s.B, s.H, s.W, s.Cin, N, cols, stages,       \
+                                                             plan.res ? 1 : 0, bias, relu, o, status)
     if (out_f32) {
         if (halo)
             PT_CONV_LAUNCH(true, true);

@@ -207,6 +207,10 @@ def main(argv=None) -> int:
     t.add_argument("--lr", type=float, default=1e-3)
     t.add_argument("--init", default=None, help="start from these weights")
     t.add_argument("--max-minutes", type=float, default=float("inf"), help="stop training after this long")
+    t.add_argument("--mix", nargs="+", default=None, metavar="KIND:FRAMES:DEFAULT:SEED0",
+                   help="per-kind training frames instead of --frames/--default-frames for all kinds: "
+                        "square frames from seeds SEED0.., default-camera frames from SEED0+500..")
+    t.add_argument("--train-seed", type=int, default=0, help="seed of the crop sampler")
     p = sub.add_parser("time")
     p.add_argument("--width", type=int, default=1920)
     p.add_argument("--height", type=int, default=1080)
@@ -231,13 +235,21 @@ def main(argv=None) -> int:
         net.sync()
         return 0
     t0 = time.perf_counter()
-    data = make_training_set(args.frames, args.size, args.target_spp, default_frames=args.default_frames)
+    if args.mix:
+        data = []
+        for spec in args.mix:
+            kind, frames, default, seed0 = spec.split(":")
+            data += make_training_set(int(frames), args.size, args.target_spp, seed0=int(seed0), kinds=(kind,),
+                                      default_frames=int(default))
+    else:
+        data = make_training_set(args.frames, args.size, args.target_spp, default_frames=args.default_frames)
     t_data = time.perf_counter() - t0
     net = UNet(seed=1)
     if args.init:
         net.set_params(load_bf16(args.init))
     t0 = time.perf_counter()
-    losses = train(net, data, args.steps, args.batch, args.crop, args.lr, max_seconds=60 * args.max_minutes)
+    losses = train(net, data, args.steps, args.batch, args.crop, args.lr, seed=args.train_seed,
+                   max_seconds=60 * args.max_minutes)
     t_train = time.perf_counter() - t0
     save_bf16(net.params(), args.out)
     np.save(os.path.splitext(args.out)[0] + "_losses.npy", np.array(losses, np.float32))

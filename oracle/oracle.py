@@ -95,12 +95,17 @@ def ref_lib() -> C.CDLL:
 
 # ---- the boxes geometry::build gives the builder (include/geometry.hpp:74-104) -------------
 def triangle_boxes(tris: np.ndarray) -> np.ndarray:
-    """triangle::bounding_box (include/triangle.hpp:76-83) in float32."""
-    pts = np.stack([tris["p0"], tris["p1"], tris["p2"]], axis=1)  # n x 3 x 3
+    """triangle::bounding_box (include/triangle.hpp:76-83) in float32, with
+    std::min / std::max over {p0, p1, p2}: the first element unless a later
+    one compares less (greater), which also decides where a NaN coordinate
+    survives (numpy's min / max would propagate every NaN)."""
+    p0, p1, p2 = (np.asarray(tris[k], np.float32) for k in ("p0", "p1", "p2"))
     pad = np.float32(1e-4)
-    lo = pts.min(axis=1) - pad
-    hi = pts.max(axis=1) + pad
-    return np.concatenate([lo, hi], axis=1).astype(np.float32)
+    lo, hi = p0.copy(), p0.copy()
+    for p in (p1, p2):
+        lo = np.where(p < lo, p, lo)
+        hi = np.where(hi < p, p, hi)
+    return np.concatenate([lo - pad, hi + pad], axis=1).astype(np.float32)
 
 
 def sphere_boxes(sph: np.ndarray) -> np.ndarray:

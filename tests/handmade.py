@@ -1,0 +1,62 @@
+"""Hand-made scene descriptions for the traversal tests (no GPU needed to
+build them)."""
+import ctypes as C
+
+import numpy as np
+
+
+def scene_from(pt, materials, spheres=(), tris=(), large=(), use_bvh=1):
+    """A small hand-made description (kept alive on the returned object)."""
+    from photon_tracer_b200 import abi
+
+    class Desc:
+        pass
+    d = Desc()
+    d.mats = (abi.pt_material * max(1, len(materials)))(*materials)
+    d.sph = (abi.pt_sphere * max(1, len(spheres)))(*spheres)
+    d.lg = (abi.pt_sphere * max(1, len(large)))(*large)
+    d.tri = (abi.pt_triangle * max(1, len(tris)))(*tris)
+    d.desc = abi.pt_scene_desc(materials=d.mats, n_materials=len(materials), spheres=d.sph, n_spheres=len(spheres),
+                               large_spheres=d.lg, n_large_spheres=len(large), triangles=d.tri, n_triangles=len(tris),
+                               use_bvh=use_bvh, sky=1, sample_lights=1)
+    d.desc_ptr = C.pointer(d.desc)
+    return d
+
+
+def tri(pt, a, b, c, mat=0):
+    from photon_tracer_b200 import abi
+    a, b, c = (np.array(x, np.float32) for x in (a, b, c))
+    e1, e2 = b - a, c - a
+    n = np.cross(e1.astype(np.float64), e2.astype(np.float64))
+    n = (n / np.linalg.norm(n)).astype(np.float32)
+    t = abi.pt_triangle(material=mat)
+    for name, v in [("p0", a), ("e1", e1), ("e2", e2), ("n0", n), ("n1", n), ("n2", n), ("face_normal", n),
+                    ("p1", b), ("p2", c)]:
+        setattr(t, name, abi.F3(*v.tolist()))
+    return t
+
+
+def non_finite_scene(pt):
+    """200 random triangles plus three with a NaN or a -1e30 coordinate, and
+    20,000 random rays through them: (description, rays)."""
+    from photon_tracer_b200 import abi
+    m = [abi.pt_material(type=0, albedo=abi.F3(0.5, 0.5, 0.5))]
+    rng = np.random.default_rng(21)
+    tris = []
+    for k in range(200):
+        c = rng.uniform(-2, 2, 3)
+        tris.append(tri(pt, c, c + rng.uniform(-0.3, 0.3, 3), c + rng.uniform(-0.3, 0.3, 3)))
+    nan = float("nan")
+    bad = [((nan, 0, 0), (1, 0, 0), (0, 1, 0)), ((0, 0, 0.2), (nan, nan, 0.2), (0, 1, 0.2)),
+           ((-1e30, 0, -0.5), (1, 0, -0.5), (0, 1, -0.5))]
+    for a, b, c in bad:
+        t = tri(pt, (0, 0, 0), (1, 0, 0), (0, 1, 0))
+        for name, v in (("p0", a), ("p1", b), ("p2", c)):
+            setattr(t, name, abi.F3(*[float(x) for x in v]))
+        e1 = np.array(b, np.float32) - np.array(a, np.float32)
+        e2 = np.array(c, np.float32) - np.array(a, np.float32)
+        t.e1, t.e2 = abi.F3(*e1.tolist()), abi.F3(*e2.tolist())
+        tris.insert(int(rng.integers(len(tris))), t)
+    d = scene_from(pt, m, (), tris)
+    rays = np.concatenate([rng.uniform(-3, 3, (20000, 3)), rng.normal(0, 1, (20000, 3))], 1).astype(np.float32)
+    return d, rays

@@ -79,6 +79,24 @@ def test_oracle_no_bvh_matches_reference(built):
     assert o.trace_closest(rays).tobytes() == r.trace_closest(rays)[0].tobytes()
 
 
+def test_oracle_non_finite_geometry_matches_reference(built):
+    """NaN and huge triangle coordinates: the oracle builds the reference's
+    trees (std::min / std::max decide where a NaN coordinate lands in a box)
+    and returns the reference's hits."""
+    from oracle.oracle import Oracle, Reference, build_trees, ref_available, reference_trees
+    if not ref_available():
+        pytest.skip("reference harness absent")
+    from handmade import non_finite_scene
+    d, rays = non_finite_scene(built)
+    r = Reference(d.desc)
+    mine, ref = build_trees(d.desc).arrays[0], reference_trees(r, d.desc).arrays[0]
+    assert mine[0].tobytes() == ref[0].tobytes() and np.array_equal(mine[1], ref[1])
+    o = Oracle(d.desc)
+    hr, bad = r.trace_closest(rays)
+    assert o.trace_closest(rays).tobytes() == hr.tobytes()
+    assert np.array_equal(o.trace_any(rays), r.trace_any(rays))
+
+
 def test_sampler_known_answers(built):
     """The Sobol pairs (sampler.hpp) of the oracle against the reference's, and
     the superset-XOR form of the second Sobol dimension the GPU computes."""

@@ -128,9 +128,21 @@ def affine_box(m: np.ndarray, t: np.ndarray, box: np.ndarray) -> np.ndarray:
             v = np.float32(np.float32(m[r, 0] * c[0]) + np.float32(m[r, 1] * c[1]))
             v = np.float32(v + np.float32(m[r, 2] * c[2]))
             p[r] = np.float32(v + t[r])
-        lo = np.minimum(lo, p)
-        hi = np.maximum(hi, p)
+        lo = np.where(p < lo, p, lo)  # aabb::grow: std::min / std::max (include/aabb.hpp:15-20)
+        hi = np.where(hi < p, p, hi)
     return np.concatenate([lo, hi])
+
+
+def _grow(vals: np.ndarray, lower: bool) -> np.float32:
+    """aabb::grow folded over vals in order, from +inf (lower) or -inf: the
+    first occurrence of the least (greatest) value that is not NaN, since a
+    NaN never compares less (greater) than the running value."""
+    v = np.asarray(vals, np.float32)
+    ok = ~np.isnan(v)
+    if not ok.any():
+        return np.float32(np.inf if lower else -np.inf)
+    best = v[ok].min() if lower else v[ok].max()
+    return v[np.nonzero(ok & (v == best))[0][0]]
 
 
 class Trees:
@@ -165,7 +177,8 @@ def build_trees(desc: abi.pt_scene_desc) -> Trees:
     for tris in a["meshes"]:
         boxes = triangle_boxes(tris)
         meshes.append(bvh_build(boxes))
-        bounds.append(np.concatenate([boxes[:, :3].min(axis=0), boxes[:, 3:].max(axis=0)]) if len(boxes) else None)
+        bounds.append(np.array([_grow(boxes[:, a], True) for a in range(3)] +
+                               [_grow(boxes[:, 3 + a], False) for a in range(3)], np.float32) if len(boxes) else None)
     flat = inst = None
     if desc.use_bvh:
         boxes = np.concatenate([sphere_boxes(a["spheres"]), triangle_boxes(a["triangles"])]) \

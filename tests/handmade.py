@@ -60,3 +60,23 @@ def non_finite_scene(pt):
     d = scene_from(pt, m, (), tris)
     rays = np.concatenate([rng.uniform(-3, 3, (20000, 3)), rng.normal(0, 1, (20000, 3))], 1).astype(np.float32)
     return d, rays
+
+
+def non_finite_instances(pt):
+    """The 150-instance scene with NaN first corners in two triangles of a
+    mesh and a -1e30 corner in a third (edges recomputed to match), and
+    20,000 random rays: (generated scene, rays). A NaN first corner makes the
+    triangle's box hold NaN, which the mesh bounds and the instance boxes
+    then skip or carry the way aabb::grow does."""
+    from photon_tracer_b200 import abi
+    g = pt.Generated(abi.PT_GEN_INSTANCES, seed=4, param=150)
+    mt = g.desc.meshes[0].triangles
+    for k in (3, 40):
+        mt[k].p0 = abi.F3(float("nan"), mt[k].p0[1], mt[k].p0[2])
+    mt[7].p2 = abi.F3(mt[7].p2[0], -1e30, mt[7].p2[2])
+    for k in (3, 40, 7):
+        p0, p1, p2 = (np.array(list(getattr(mt[k], n)), np.float32) for n in ("p0", "p1", "p2"))
+        mt[k].e1 = abi.F3(*(p1 - p0).tolist())
+        mt[k].e2 = abi.F3(*(p2 - p0).tolist())
+    rays = pt.generate_rays(4, [-40, -1, -40], [40, 30, 40], 20000)
+    return g, rays

@@ -80,9 +80,9 @@ def test_oracle_no_bvh_matches_reference(built):
 
 
 def test_oracle_non_finite_geometry_matches_reference(built):
-    """NaN and huge triangle coordinates: the oracle builds the reference's
-    trees (std::min / std::max decide where a NaN coordinate lands in a box)
-    and returns the reference's hits."""
+    """NaN and huge triangle coordinates, flat and instanced: the oracle
+    builds the reference's trees (std::min / std::max decide where a NaN
+    coordinate lands in a box) and returns the reference's hits."""
     from oracle.oracle import Oracle, Reference, build_trees, ref_available, reference_trees
     if not ref_available():
         pytest.skip("reference harness absent")
@@ -94,6 +94,16 @@ def test_oracle_non_finite_geometry_matches_reference(built):
     o = Oracle(d.desc)
     hr, bad = r.trace_closest(rays)
     assert o.trace_closest(rays).tobytes() == hr.tobytes()
+    assert np.array_equal(o.trace_any(rays), r.trace_any(rays))
+    # instances of a mesh with NaN in triangle boxes: mesh bounds and instance
+    # boxes as aabb::grow makes them
+    from handmade import non_finite_instances
+    g, rays = non_finite_instances(built)
+    r = Reference(g.desc)
+    for mine, ref in zip(build_trees(g.desc).arrays, reference_trees(r, g.desc).arrays):
+        assert mine[0].tobytes() == ref[0].tobytes() and np.array_equal(mine[1], ref[1])
+    o = Oracle(g.desc)
+    assert o.trace_closest(rays).tobytes() == r.trace_closest(rays)[0].tobytes()
     assert np.array_equal(o.trace_any(rays), r.trace_any(rays))
 
 

@@ -30,6 +30,13 @@ constexpr int kTileW = 8, kTileH = 4;
 // The pixel coordinates, sample number and running sum of each lane in
 // shared memory instead of registers (they change once per path): 170 -> 100
 // bytes of spills in the flat-scene form, room frame +0.8%, images identical.
+// The path state of each lane in shared memory in the flat-scene form: no
+// spills left there, room frame +1.0%, random spheres +3.7%; the instanced
+// form lost 3% with it and keeps registers (the RNG state moved as well
+// gained nothing more).
+#ifndef PT_MEGA_SMEM_PATH
+#define PT_MEGA_SMEM_PATH 1
+#endif
 #ifndef PT_MEGA_SMEM_STATE
 #define PT_MEGA_SMEM_STATE 1
 #endif
@@ -74,7 +81,12 @@ __global__ void __launch_bounds__(128, PT_MEGA_MIN_BLOCKS) megakernel(PtSceneDev
     V acc = mk(0, 0, 0), acc_albedo = mk(0, 0, 0), acc_normal = mk(0, 0, 0);
 #endif
     float lum2 = 0;
-    Path path;
+    // Flat-scene form: the path (ray, throughput, radiance, bounce) in shared
+    // memory too, read into registers where a query or shading needs it.
+    constexpr bool SMEM_PATH = PT_MEGA_SMEM_PATH && TREES == PT_TREES_FLAT;
+    __shared__ Path s_path[SMEM_PATH ? 128 : 1];
+    Path local_path;
+    Path& path = SMEM_PATH ? s_path[threadIdx.x] : local_path;
     First first = {mk(0, 0, 0), mk(0, 0, 0)};
     Sampler smp;
     Rng rng;

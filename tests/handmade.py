@@ -80,3 +80,23 @@ def non_finite_instances(pt):
         mt[k].e2 = abi.F3(*(p2 - p0).tolist())
     rays = pt.generate_rays(4, [-40, -1, -40], [40, 30, 40], 20000)
     return g, rays
+
+
+def non_finite_spheres(pt):
+    """100 random spheres with a NaN centre, a NaN radius and a 1e30 centre
+    among them, a ground sphere and a NaN-centred large sphere, and 20,000
+    random rays: (description, rays)."""
+    from photon_tracer_b200 import abi
+    m = [abi.pt_material(type=0, albedo=abi.F3(0.5, 0.5, 0.5))]
+    rng = np.random.default_rng(5)
+    sph = [abi.pt_sphere(center=abi.F3(*rng.uniform(-2, 2, 3).tolist()), radius=float(rng.uniform(0.1, 0.4)))
+           for _ in range(100)]
+    nan = float("nan")
+    sph[10] = abi.pt_sphere(center=abi.F3(nan, 0, 0), radius=0.3)
+    sph[50] = abi.pt_sphere(center=abi.F3(0, 0, 0), radius=nan)
+    sph[70] = abi.pt_sphere(center=abi.F3(0.5, 1e30, 0), radius=0.2)
+    large = [abi.pt_sphere(center=abi.F3(0, -1001, 0), radius=1000.0),
+             abi.pt_sphere(center=abi.F3(nan, 0, 0), radius=1000.0)]
+    d = scene_from(pt, m, sph, [tri(pt, (0, 0, 0), (1, 0, 0), (0, 1, 0))], large)
+    rays = np.concatenate([rng.uniform(-3, 3, (20000, 3)), rng.normal(0, 1, (20000, 3))], 1).astype(np.float32)
+    return d, rays

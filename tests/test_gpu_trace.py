@@ -7,7 +7,8 @@ import numpy as np
 import pytest
 
 from conftest import GOLDEN, golden
-from handmade import non_finite_instances, non_finite_scene, scene_from as _scene_from, tri as _tri
+from handmade import non_finite_instances, non_finite_scene, non_finite_spheres
+from handmade import scene_from as _scene_from, tri as _tri
 
 pytestmark = pytest.mark.gpu
 
@@ -169,6 +170,11 @@ def test_non_finite_geometry(pt):
     g, rays = non_finite_instances(pt)
     s = pt.Scene(g)
     o = Oracle(g.desc)
+    assert_hits_equal(s.trace_closest(rays), o.trace_closest(rays), rays)
+    assert np.array_equal(s.trace_any(rays), o.trace_any(rays))
+    d, rays = non_finite_spheres(pt)
+    s = pt.Scene(d.desc_ptr)
+    o = Oracle(d.desc)
     assert_hits_equal(s.trace_closest(rays), o.trace_closest(rays), rays)
     assert np.array_equal(s.trace_any(rays), o.trace_any(rays))
 

@@ -105,6 +105,15 @@ def test_oracle_non_finite_geometry_matches_reference(built):
     o = Oracle(g.desc)
     assert o.trace_closest(rays).tobytes() == r.trace_closest(rays)[0].tobytes()
     assert np.array_equal(o.trace_any(rays), r.trace_any(rays))
+    # spheres and a large sphere with NaN or huge centres and radii
+    from handmade import non_finite_spheres
+    d, rays = non_finite_spheres(built)
+    r = Reference(d.desc)
+    mine, ref = build_trees(d.desc).arrays[0], reference_trees(r, d.desc).arrays[0]
+    assert mine[0].tobytes() == ref[0].tobytes() and np.array_equal(mine[1], ref[1])
+    o = Oracle(d.desc)
+    assert o.trace_closest(rays).tobytes() == r.trace_closest(rays)[0].tobytes()
+    assert np.array_equal(o.trace_any(rays), r.trace_any(rays))
 
 
 def test_sampler_known_answers(built):

@@ -36,6 +36,22 @@ def tri(pt, a, b, c, mat=0):
     return t
 
 
+def set_corners(t, a, b, c):
+    """Corners a, b, c with the edges and face normal the reference's
+    triangle constructor derives from them (float32, its evaluation order:
+    e = corner - p0, face normal = cross(e1, e2) / its length per component)."""
+    from photon_tracer_b200 import abi
+    p0, p1, p2 = (np.array(x, np.float32) for x in (a, b, c))
+    e1, e2 = p1 - p0, p2 - p0
+    n = np.array([e1[1] * e2[2] - e1[2] * e2[1], e1[2] * e2[0] - e1[0] * e2[2], e1[0] * e2[1] - e1[1] * e2[0]],
+                 np.float32)
+    with np.errstate(all="ignore"):
+        length = np.sqrt(np.float32(n[0] * n[0] + n[1] * n[1]) + n[2] * n[2], dtype=np.float32)
+        n = (n / length).astype(np.float32)
+    for name, v in (("p0", p0), ("p1", p1), ("p2", p2), ("e1", e1), ("e2", e2), ("face_normal", n)):
+        setattr(t, name, abi.F3(*v.tolist()))
+
+
 def non_finite_scene(pt):
     """200 random triangles plus three with a NaN or a -1e30 coordinate, and
     20,000 random rays through them: (description, rays)."""
@@ -45,17 +61,15 @@ def non_finite_scene(pt):
     tris = []
     for k in range(200):
         c = rng.uniform(-2, 2, 3)
-        tris.append(tri(pt, c, c + rng.uniform(-0.3, 0.3, 3), c + rng.uniform(-0.3, 0.3, 3)))
+        t = tri(pt, (0, 0, 0), (1, 0, 0), (0, 1, 0))
+        set_corners(t, c, c + rng.uniform(-0.3, 0.3, 3), c + rng.uniform(-0.3, 0.3, 3))
+        tris.append(t)
     nan = float("nan")
     bad = [((nan, 0, 0), (1, 0, 0), (0, 1, 0)), ((0, 0, 0.2), (nan, nan, 0.2), (0, 1, 0.2)),
            ((-1e30, 0, -0.5), (1, 0, -0.5), (0, 1, -0.5))]
     for a, b, c in bad:
         t = tri(pt, (0, 0, 0), (1, 0, 0), (0, 1, 0))
-        for name, v in (("p0", a), ("p1", b), ("p2", c)):
-            setattr(t, name, abi.F3(*[float(x) for x in v]))
-        e1 = np.array(b, np.float32) - np.array(a, np.float32)
-        e2 = np.array(c, np.float32) - np.array(a, np.float32)
-        t.e1, t.e2 = abi.F3(*e1.tolist()), abi.F3(*e2.tolist())
+        set_corners(t, a, b, c)
         tris.insert(int(rng.integers(len(tris))), t)
     d = scene_from(pt, m, (), tris)
     rays = np.concatenate([rng.uniform(-3, 3, (20000, 3)), rng.normal(0, 1, (20000, 3))], 1).astype(np.float32)
@@ -64,20 +78,21 @@ def non_finite_scene(pt):
 
 def non_finite_instances(pt):
     """The 150-instance scene with NaN first corners in two triangles of a
-    mesh and a -1e30 corner in a third (edges recomputed to match), and
+    mesh and a -1e30 corner in a third (edges and face normals recomputed
+    to match), and
     20,000 random rays: (generated scene, rays). A NaN first corner makes the
     triangle's box hold NaN, which the mesh bounds and the instance boxes
     then skip or carry the way aabb::grow does."""
     from photon_tracer_b200 import abi
     g = pt.Generated(abi.PT_GEN_INSTANCES, seed=4, param=150)
     mt = g.desc.meshes[0].triangles
-    for k in (3, 40):
-        mt[k].p0 = abi.F3(float("nan"), mt[k].p0[1], mt[k].p0[2])
-    mt[7].p2 = abi.F3(mt[7].p2[0], -1e30, mt[7].p2[2])
     for k in (3, 40, 7):
-        p0, p1, p2 = (np.array(list(getattr(mt[k], n)), np.float32) for n in ("p0", "p1", "p2"))
-        mt[k].e1 = abi.F3(*(p1 - p0).tolist())
-        mt[k].e2 = abi.F3(*(p2 - p0).tolist())
+        p0, p1, p2 = (list(getattr(mt[k], n)) for n in ("p0", "p1", "p2"))
+        if k == 7:
+            p2[1] = -1e30
+        else:
+            p0[0] = float("nan")
+        set_corners(mt[k], p0, p1, p2)
     rays = pt.generate_rays(4, [-40, -1, -40], [40, 30, 40], 20000)
     return g, rays
 

@@ -83,6 +83,30 @@ def test_sample_stream_render_matches_oracle(pt, kind, param, w, h, spp):
     assert abs(int(rays) - int(rrays)) <= 0.01 * int(rrays)
 
 
+def test_non_finite_scenes_render_like_oracle(pt):
+    """Scenes with NaN or huge triangle and sphere coordinates, flat and
+    instanced (their node boxes are not all ordered, so every ray takes the
+    exact SSE-emulating slab test): GPU renders against the oracle's, whose
+    renders of the same scenes equal the reference's (tests/test_oracle.py)."""
+    from handmade import non_finite_instances, non_finite_scene, non_finite_spheres
+    from oracle.oracle import Oracle
+    from photon_tracer_b200 import abi
+    cam = pt.camera_look_at((0.0, 0.5, 6.0), (0.0, 0.0, 0.0), 50.0, 1.5)
+    tris, spheres, g = non_finite_scene(pt)[0], non_finite_spheres(pt)[0], non_finite_instances(pt)[0]
+    for what, scene, desc, c in (("triangles", tris.desc_ptr, tris.desc, cam),
+                                 ("spheres", spheres.desc_ptr, spheres.desc, cam),
+                                 ("instances", g, g.desc, g.camera)):
+        s = pt.Scene(scene)
+        img, aux, rays = s.render(c, 48, 32, 4, 10, seed=9, aux=True, mode=abi.PT_MODE_MEGAKERNEL)
+        ref, raux, rrays = Oracle(desc).render(c, 48, 32, 4, 10, seed=9, rng_mode=0, aux=True)
+        # a NaN triangle's normal is NaN in the aux guides: same pixels, then
+        # the rest within the render tolerance
+        assert np.array_equal(np.isnan(img), np.isnan(ref)) and np.array_equal(np.isnan(aux), np.isnan(raux))
+        assert_render_close(np.nan_to_num(img), np.nan_to_num(ref), what)
+        assert_render_close(np.nan_to_num(aux), np.nan_to_num(raux), what + " aux")
+        assert abs(int(rays) - int(rrays)) <= 0.01 * int(rrays)
+
+
 def test_render_is_deterministic_and_row_call_agrees(pt):
     """Same seed, same bytes; render_row_linear(j) equals row H-1-j of the frame."""
     from photon_tracer_b200 import abi

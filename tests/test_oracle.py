@@ -80,13 +80,14 @@ def test_oracle_no_bvh_matches_reference(built):
 
 
 def test_oracle_non_finite_geometry_matches_reference(built):
-    """NaN and huge triangle coordinates, flat and instanced: the oracle
-    builds the reference's trees (std::min / std::max decide where a NaN
-    coordinate lands in a box) and returns the reference's hits."""
+    """NaN and huge coordinates in triangles (flat and instanced) and
+    spheres: the oracle builds the reference's trees (std::min / std::max
+    decide where a NaN coordinate lands in a box) and returns the
+    reference's hits and renders."""
     from oracle.oracle import Oracle, Reference, build_trees, ref_available, reference_trees
     if not ref_available():
         pytest.skip("reference harness absent")
-    from handmade import non_finite_scene
+    from handmade import non_finite_instances, non_finite_scene, non_finite_spheres
     d, rays = non_finite_scene(built)
     r = Reference(d.desc)
     mine, ref = build_trees(d.desc).arrays[0], reference_trees(r, d.desc).arrays[0]
@@ -97,7 +98,6 @@ def test_oracle_non_finite_geometry_matches_reference(built):
     assert np.array_equal(o.trace_any(rays), r.trace_any(rays))
     # instances of a mesh with NaN in triangle boxes: mesh bounds and instance
     # boxes as aabb::grow makes them
-    from handmade import non_finite_instances
     g, rays = non_finite_instances(built)
     r = Reference(g.desc)
     for mine, ref in zip(build_trees(g.desc).arrays, reference_trees(r, g.desc).arrays):
@@ -106,7 +106,6 @@ def test_oracle_non_finite_geometry_matches_reference(built):
     assert o.trace_closest(rays).tobytes() == r.trace_closest(rays)[0].tobytes()
     assert np.array_equal(o.trace_any(rays), r.trace_any(rays))
     # spheres and a large sphere with NaN or huge centres and radii
-    from handmade import non_finite_spheres
     d, rays = non_finite_spheres(built)
     r = Reference(d.desc)
     mine, ref = build_trees(d.desc).arrays[0], reference_trees(r, d.desc).arrays[0]
@@ -114,6 +113,14 @@ def test_oracle_non_finite_geometry_matches_reference(built):
     o = Oracle(d.desc)
     assert o.trace_closest(rays).tobytes() == r.trace_closest(rays)[0].tobytes()
     assert np.array_equal(o.trace_any(rays), r.trace_any(rays))
+    # whole renders through all three scenes: same images, guides and ray counts
+    cam = built.camera_look_at((0.0, 0.5, 6.0), (0.0, 0.0, 0.0), 50.0, 1.5)
+    for desc, c in ((non_finite_scene(built)[0].desc, cam), (non_finite_spheres(built)[0].desc, cam),
+                    (g.desc, g.camera)):
+        o, r = Oracle(desc), Reference(desc)
+        io, ao, ro = o.render(c, 24, 16, 3, 10, seed=3, rng_mode=2, aux=True)
+        ir, ar, rr = r.render(c, 24, 16, 3, 10, seed=3, aux=True)
+        assert io.tobytes() == ir.tobytes() and ao.tobytes() == ar.tobytes() and ro == rr
 
 
 def test_sampler_known_answers(built):

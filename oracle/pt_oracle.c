@@ -261,6 +261,12 @@ static void traverse(const tree* tr, v3 o, v3 d, float t_min, float* t_max, coun
             for (; k > 0 && hit[k - 1].t < h.t; --k) hit[k] = hit[k - 1];
             hit[k] = h;
         }
+        /* bvh.hpp pushes without a bound; 3 * depth + 1 entries suffice for
+           every ray whose slab values are not NaN. A NaN origin or direction
+           makes every child test pass, empty children (first 0, count 0)
+           included, which re-enter the root without end: the reference then
+           overruns its stack and crashes. Here the walk stops instead. */
+        if (top + n > PO_STACK) return;
         for (k = 0; k < n; ++k) stack[top++] = hit[k];
     }
 }

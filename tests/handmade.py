@@ -115,3 +115,21 @@ def non_finite_spheres(pt):
     d = scene_from(pt, m, sph, [tri(pt, (0, 0, 0), (1, 0, 0), (0, 1, 0))], large)
     rays = np.concatenate([rng.uniform(-3, 3, (20000, 3)), rng.normal(0, 1, (20000, 3))], 1).astype(np.float32)
     return d, rays
+
+
+def adversarial_rays(seed, n, nan=False):
+    """Random rays in [-3, 3]^6 with 15% of their components replaced by
+    infinities, signed zeros, denormals or +-1e38 (and NaN when nan=True)."""
+    rng = np.random.default_rng(seed)
+    vals = [np.inf, -np.inf, 0.0, -0.0, 1e-45, -1e-45, 1e38, -1e38, 1.0, -1.0, 0.5] + ([np.nan] if nan else [])
+    vals = np.array(vals, np.float32)
+    rays = rng.uniform(-3, 3, (n, 6)).astype(np.float32)
+    mask = rng.random((n, 6)) < 0.15
+    rays[mask] = vals[rng.integers(len(vals), size=int(mask.sum()))]
+    return rays
+
+
+# A ray with a NaN origin: every slab test passes, empty child slots (first 0)
+# re-enter the root, and the walk never ends; the reference overruns its
+# stack on it.
+NAN_ORIGIN_RAY = np.array([[-1.636903, np.nan, np.nan, 0.6391732, -0.9654722, 2.588736]], np.float32)

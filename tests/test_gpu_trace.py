@@ -7,6 +7,7 @@ import numpy as np
 import pytest
 
 from conftest import GOLDEN, golden
+from handmade import NAN_ORIGIN_RAY, adversarial_rays
 from handmade import non_finite_instances, non_finite_scene, non_finite_spheres
 from handmade import scene_from as _scene_from, tri as _tri
 
@@ -177,6 +178,29 @@ def test_non_finite_geometry(pt):
     o = Oracle(d.desc)
     assert_hits_equal(s.trace_closest(rays), o.trace_closest(rays), rays)
     assert np.array_equal(s.trace_any(rays), o.trace_any(rays))
+
+
+def test_adversarial_rays(pt):
+    """Rays with infinite, signed-zero, denormal and huge components match
+    the oracle bit for bit (which matches the reference on them,
+    tests/test_oracle.py). A ray with a NaN origin, on which the reference's
+    walk never ends, makes the call fail with PT_ERR_STACK_OVERFLOW (the
+    stack bound is checked on every push), and the scene stays usable."""
+    from oracle.oracle import Oracle
+    from photon_tracer_b200 import abi
+    rays = adversarial_rays(9, 20000)
+    for kind, param in ((abi.PT_GEN_ROOM_MESH, 3), (abi.PT_GEN_INSTANCES, 150), (abi.PT_GEN_REF_MATERIALS, 0)):
+        g = pt.Generated(kind, seed=2, param=param)
+        s = pt.Scene(g)
+        o = Oracle(g.desc)
+        assert_hits_equal(s.trace_closest(rays), o.trace_closest(rays), rays)
+        assert np.array_equal(s.trace_any(rays), o.trace_any(rays))
+    g = pt.Generated(abi.PT_GEN_ROOM_MESH, seed=2, param=3)
+    s = pt.Scene(g)
+    with pytest.raises(abi.PhotonError) as e:
+        s.trace_closest(NAN_ORIGIN_RAY)
+    assert e.value.status == abi.PT_ERR_STACK_OVERFLOW
+    assert_hits_equal(s.trace_closest(rays), Oracle(g.desc).trace_closest(rays), rays)
 
 
 def test_device_buffers_entry_point(pt):

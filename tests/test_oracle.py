@@ -123,6 +123,25 @@ def test_oracle_non_finite_geometry_matches_reference(built):
         assert io.tobytes() == ir.tobytes() and ao.tobytes() == ar.tobytes() and ro == rr
 
 
+def test_oracle_adversarial_rays_match_reference(built):
+    """Rays with infinite, signed-zero, denormal and huge components: oracle
+    = reference, closest and any hit. Rays with NaN components send the
+    reference's walk round the root without end (it crashes); the oracle
+    stops its walk at the stack bound instead, and must survive them."""
+    from handmade import NAN_ORIGIN_RAY, adversarial_rays
+    from oracle.oracle import Oracle, Reference, ref_available
+    from photon_tracer_b200 import abi
+    rays = adversarial_rays(9, 20000)
+    for kind, param in ((abi.PT_GEN_ROOM_MESH, 3), (abi.PT_GEN_INSTANCES, 150), (abi.PT_GEN_REF_MATERIALS, 0)):
+        g = built.Generated(kind, seed=2, param=param)
+        o = Oracle(g.desc)
+        o.trace_closest(np.concatenate([adversarial_rays(10, 2000, nan=True), NAN_ORIGIN_RAY]))
+        if ref_available():
+            r = Reference(g.desc)
+            assert o.trace_closest(rays).tobytes() == r.trace_closest(rays)[0].tobytes()
+            assert np.array_equal(o.trace_any(rays), r.trace_any(rays))
+
+
 def test_sampler_known_answers(built):
     """The Sobol pairs (sampler.hpp) of the oracle against the reference's, and
     the superset-XOR form of the second Sobol dimension the GPU computes."""

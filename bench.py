@@ -213,7 +213,7 @@ def run_profile_case(args):
 
 
 def run_batch_workload(args):
-    """64 scenes (batch generator seeds 1..64) in one
+    """The 64-scene batch (batch generator seeds 1..64) in one
     persistent launch from a CUDA graph, the strategy picked by the
     autotuner, against one megakernel launch per scene."""
     import torch
@@ -399,7 +399,8 @@ def run_bvh_workload(args):
 
 
 def run_scene_workload(args, kind, label, param=0):
-    """Mrays/s of the megakernel on another BASELINE configuration."""
+    """Mrays/s of the megakernel on another benchmark scene (instances or
+    random spheres)."""
     import torch
     import photon_tracer_b200 as pt
     from photon_tracer_b200 import abi
@@ -440,7 +441,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default="room",
                     choices=["room", "batch", "convergence", "unet", "bvh", "instances", "spheres"],
-                    help="room: the headline line (config 1); the others print their own JSON line")
+                    help="room: the headline line (room + displaced icosphere, 1024x1024, 64 spp); "
+                         "the others print their own JSON line")
     ap.add_argument("--seeds", type=int, nargs="+", default=[1001, 1002])
     ap.add_argument("--kinds", nargs="+", default=["spheres", "room", "instances"],
                     help="convergence: scene generators (random spheres, room mesh, instancing)")

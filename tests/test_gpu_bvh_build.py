@@ -82,7 +82,7 @@ def test_signed_zeros(pt):
 
 
 def test_mesh_triangles(pt):
-    """Triangle boxes of the displaced icosphere (config 1's mesh, 81,920
+    """Triangle boxes of the displaced icosphere (the room scene's mesh, 81,920
     triangles), in the generator's order."""
     from photon_tracer_b200 import abi
     g = pt.Generated(abi.PT_GEN_ROOM_MESH, seed=1)

@@ -1,4 +1,4 @@
-"""TEST INFRASTRUCTURE: builds the checkers the tests use.
+"""TEST INFRASTRUCTURE: builds the libraries the tests compare against.
 
 * oracle/libptoracle.so -- the plain-C restatement (pt_oracle.c), always.
 * oracle/_ref/libptref.so -- the reference itself: ref_harness.cpp compiled

@@ -2,7 +2,7 @@
  * pt_oracle.c -- TEST INFRASTRUCTURE, not part of the product.
  *
  * A plain-C, single-threaded CPU restatement of photon_tracer's render hot
- * path, used only as the checker by tests/, __graft_entry__.smoke() and the
+ * path, used only to check results in tests/, __graft_entry__.smoke() and the
  * CPU-baseline leg of bench.py. Nothing in the product links or calls it.
  *
  * Each function names the reference function it restates (photon_tracer,

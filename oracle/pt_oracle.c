@@ -668,9 +668,10 @@ static int scatter(const pt_material* m, v3 d_in, const rec_t* rec, const sample
         *att = ld3(m->albedo);
         return 1;
     }
-    if (m->type == PT_MAT_METAL) { /* :85-91 */
+    if (m->type == PT_MAT_METAL) { /* :85-91; the constructor keeps fuzz = f < 1 ? f : 1 (:83) */
+        const float fuzz = m->fuzz < 1 ? m->fuzz : 1;
         v3 refl = reflect(normalize(d_in), rec->normal);
-        *dir = add(refl, scl(random_in_unit_sphere(r), m->fuzz));
+        *dir = add(refl, scl(random_in_unit_sphere(r), fuzz));
         *att = ld3(m->albedo);
         return dot(*dir, rec->normal) > 0;
     }

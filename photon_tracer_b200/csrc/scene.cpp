@@ -171,7 +171,8 @@ pt_status build_arena(const pt_scene_desc& d, HostArena& A) {
         if (m.type == PT_MAT_DIELECTRIC) flags |= PT_MF_TRANSMISSIVE;
         PtMaterial g;
         g.albedo_type = make_float4(m.albedo[0], m.albedo[1], m.albedo[2], ubits(m.type));
-        g.emission_fuzz = make_float4(m.emission[0], m.emission[1], m.emission[2], m.fuzz);
+        // metal keeps fuzz = f < 1 ? f : 1 (include/material.hpp:83; NaN becomes 1)
+        g.emission_fuzz = make_float4(m.emission[0], m.emission[1], m.emission[2], m.fuzz < 1.0f ? m.fuzz : 1.0f);
         // only lambertians are textured (lambertian::texture, include/material.hpp:50)
         const bool textured = m.type == PT_MAT_LAMBERTIAN && m.texture > 0;
         g.ior_flags = make_float4(m.ior, ubits(flags), ubits(textured ? m.texture - 1 : PT_NONE), 0);

@@ -133,3 +133,30 @@ def adversarial_rays(seed, n, nan=False):
 # re-enter the root, and the walk never ends; the reference overruns its
 # stack on it.
 NAN_ORIGIN_RAY = np.array([[-1.636903, np.nan, np.nan, 0.6391732, -0.9654722, 2.588736]], np.float32)
+
+
+def random_material_scene(pt, seed):
+    """Eight random materials of all four kinds (metal fuzz up to 1.7, which
+    the reference clamps to 1; dielectric ior 0.7 to 2.4), 20 spheres (some
+    with a negative radius), 30 triangles and a ground sphere, and a camera:
+    (description, camera)."""
+    from photon_tracer_b200 import abi
+    rng = np.random.default_rng(seed)
+    mats = []
+    for k in range(8):
+        t = int(rng.integers(4))
+        mats.append(abi.pt_material(type=t, albedo=abi.F3(*rng.uniform(0, 1, 3).tolist()),
+                                    emission=abi.F3(*(rng.uniform(0, 4, 3) if t == 3 else np.zeros(3)).tolist()),
+                                    fuzz=float(rng.choice([0.0, 0.3, 1.0, 1.7])),
+                                    ior=float(rng.choice([1.0, 1.5, 0.7, 2.4]))))
+    sph = [abi.pt_sphere(center=abi.F3(*rng.uniform(-2, 2, 3).tolist()), radius=float(rng.choice([0.3, 0.6, -0.4])),
+                         material=int(rng.integers(8))) for _ in range(20)]
+    tris = []
+    for _ in range(30):
+        c = rng.uniform(-2, 2, 3)
+        t = tri(pt, (0, 0, 0), (1, 0, 0), (0, 1, 0), mat=int(rng.integers(8)))
+        set_corners(t, c, c + rng.uniform(-0.8, 0.8, 3), c + rng.uniform(-0.8, 0.8, 3))
+        tris.append(t)
+    large = [abi.pt_sphere(center=abi.F3(0, -1001, 0), radius=1000.0, material=int(rng.integers(8)))]
+    cam = pt.camera_look_at(tuple(rng.uniform(-5, 5, 3).tolist()), (0.0, 0.0, 0.0), 40.0, 1.5)
+    return scene_from(pt, mats, sph, tris, large), cam

@@ -304,6 +304,13 @@ pt_status pt_primary_depth_device(pt_scene* scene, const pt_camera* cam, int wid
  * pt_trace_closest. counts[5] = {nodes, order, triangles, spheres, instances}. */
 pt_status pt_trace_count(pt_scene* scene, const float* rays, size_t n, float tmin, float tmax, uint64_t counts[5]);
 
+/* ---- instance transforms (host) -------------------------------------------- */
+/* affine::inverse (include/transform.hpp:42-59): cofactors and determinant in
+ * double, the linear part rounded to float, t = -(M^-1 t) in float. This is the
+ * to_object a pt_instance must carry for its to_world. A singular to_world
+ * gives infinite or NaN entries, as in the reference. */
+pt_status pt_affine_inverse(const pt_affine* to_world, pt_affine* to_object);
+
 /* ---- BVH build (host) ------------------------------------------------------ */
 /* The library's own host builder: binned SAH (16 bins, leaf <= 8, depth <= 64)
  * collapsed to 4-wide nodes, producing the same nodes and order as

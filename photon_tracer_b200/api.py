@@ -67,6 +67,13 @@ def generate_rays(seed: int, lo, hi, n: int) -> np.ndarray:
 
 
 # ---- BVH --------------------------------------------------------------------------
+def affine_inverse(to_world: "abi.pt_affine") -> "abi.pt_affine":
+    """The to_object an instance must carry for to_world (affine::inverse)."""
+    out = abi.pt_affine()
+    check(load().pt_affine_inverse(C.byref(to_world), C.byref(out)))
+    return out
+
+
 def bvh_build(boxes: np.ndarray, gpu: bool = False):
     """The library's builder (same nodes and order as the reference's bvh::build).
     boxes: (n, 6) float32 min xyz, max xyz. Returns (nodes structured array, order).

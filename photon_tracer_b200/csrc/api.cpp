@@ -190,6 +190,13 @@ const char* pt_version(void) { return "photon_cuda 0.1 (sm_100a)"; }
 
 void pt_free(void* p) { std::free(p); }
 
+pt_status pt_affine_inverse(const pt_affine* to_world, pt_affine* to_object) {
+    clear_error();
+    if (!to_world || !to_object) return fail(PT_ERR_INVALID_ARG, "pt_affine_inverse: null pointer");
+    *to_object = affine_inverse(*to_world);
+    return PT_OK;
+}
+
 pt_status pt_bvh_build(const float* boxes, uint32_t n, pt_bvh_node** nodes, uint32_t* n_nodes, uint32_t** order) {
     clear_error();
     if ((!boxes && n) || !nodes || !n_nodes || !order) return fail(PT_ERR_INVALID_ARG, "pt_bvh_build: null pointer");

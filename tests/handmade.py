@@ -160,3 +160,30 @@ def random_material_scene(pt, seed):
     large = [abi.pt_sphere(center=abi.F3(0, -1001, 0), radius=1000.0, material=int(rng.integers(8)))]
     cam = pt.camera_look_at(tuple(rng.uniform(-5, 5, 3).tolist()), (0.0, 0.0, 0.0), 40.0, 1.5)
     return scene_from(pt, mats, sph, tris, large), cam
+
+
+def random_transform_instances(pt, seed, singular=False):
+    """The 60-instance scene with every to_world replaced by a random rotation
+    times per-axis scales from {0.5, 1, 2, -1, 1e-3} (mirrors and flattening
+    included; instance 9 scaled by 1e-20; with singular=True instance 5's
+    last row zeroed) and to_object from pt.affine_inverse: the generated
+    scene."""
+    from photon_tracer_b200 import abi
+    rng = np.random.default_rng(seed)
+    g = pt.Generated(abi.PT_GEN_INSTANCES, seed=4, param=60)
+    d = g.desc
+    for k in range(d.n_instances):
+        q, _ = np.linalg.qr(rng.normal(size=(3, 3)))
+        m = (q * rng.choice([0.5, 1.0, 2.0, -1.0, 1e-3], 3)).astype(np.float32)
+        if k == 9:
+            m = np.eye(3, dtype=np.float32) * np.float32(1e-20)
+        if singular and k == 5:
+            m[2] = 0
+        t = rng.uniform(-30, 30, 3).astype(np.float32)
+        inst = d.instances[k]
+        for r in range(3):
+            for c in range(3):
+                inst.to_world.m[r][c] = float(m[r, c])
+            inst.to_world.t[r] = float(t[r])
+        inst.to_object = pt.affine_inverse(inst.to_world)
+    return g

@@ -159,6 +159,35 @@ def test_oracle_random_materials_match_reference(built):
         assert io.tobytes() == ir.tobytes() and ao.tobytes() == ar.tobytes() and ro == rr, seed
 
 
+def test_instance_transforms_match_reference(built):
+    """pt_affine_inverse gives the reference's affine::inverse bit for bit
+    (singular matrices included: infinities and NaN alike), and with it the
+    oracle traces and renders instances under random rotations, mirrors,
+    flattening and a 1e-20 scale as the reference does."""
+    import ctypes as C
+    from handmade import random_transform_instances
+    from oracle.oracle import Oracle, Reference, ref_available
+    if not ref_available():
+        pytest.skip("reference harness absent")
+    out = (C.c_float * 12)()
+    for singular in (True, False):
+        g = random_transform_instances(built, 3, singular)
+        d = g.desc
+        r = Reference(d)
+        for k in range(d.n_instances):
+            r.lib.ref_instance_to_object(r.h, k, out)
+            x = d.instances[k].to_object
+            mine = [x.m[i][j] for i in range(3) for j in range(3)] + list(x.t)
+            assert np.array(mine, np.float32).tobytes() == np.array(out[:], np.float32).tobytes(), k
+    o = Oracle(d)
+    rays = built.generate_rays(4, [-40, -1, -40], [40, 30, 40], 20000)
+    assert o.trace_closest(rays).tobytes() == r.trace_closest(rays)[0].tobytes()
+    assert np.array_equal(o.trace_any(rays), r.trace_any(rays))
+    io, ao, ro = o.render(g.camera, 24, 16, 3, 10, seed=3, rng_mode=2, aux=True)
+    ir, ar, rr = r.render(g.camera, 24, 16, 3, 10, seed=3, aux=True)
+    assert io.tobytes() == ir.tobytes() and ao.tobytes() == ar.tobytes() and ro == rr
+
+
 def test_sampler_known_answers(built):
     """The Sobol pairs (sampler.hpp) of the oracle against the reference's, and
     the superset-XOR form of the second Sobol dimension the GPU computes."""

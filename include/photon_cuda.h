@@ -56,8 +56,9 @@ enum { PT_MAT_LAMBERTIAN = 0, PT_MAT_METAL = 1, PT_MAT_DIELECTRIC = 2, PT_MAT_DI
 #define PT_NO_MATERIAL 0xffffffffu
 
 /* One material: include/material.hpp:13-30 (emission, diffuse, transmissive)
- * plus the subclass fields (albedo :48, fuzz :81 (already clamped to <= 1),
- * ior :109). diffuse/transmissive follow from type. */
+ * plus the subclass fields (albedo :48, fuzz :81 -- the library applies the
+ * metal constructor's clamp f < 1 ? f : 1 (:83) --, ior :109).
+ * diffuse/transmissive follow from type. */
 typedef struct pt_material {
     uint32_t type;
     float albedo[3];
@@ -87,8 +88,9 @@ typedef struct pt_sphere {
  * reference's constructor computed them (e1 = p1 - p0, e2 = p2 - p0,
  * face_normal = normalize(cross(e1, e2)); vertex normals = face normal for
  * a flat triangle). p1 and p2 are the corners as given, which the bounding
- * box (include/triangle.hpp:76-83) is taken from. Texture coordinates are
- * not carried. */
+ * box (include/triangle.hpp:76-83) is taken from. uv holds the texture
+ * coordinates at the three corners. pt_triangle_init fills the derived
+ * fields the reference's way. */
 typedef struct pt_triangle {
     float p0[3], e1[3], e2[3];
     float n0[3], n1[3], n2[3];
@@ -303,6 +305,14 @@ pt_status pt_primary_depth_device(pt_scene* scene, const pt_camera* cam, int wid
  * instances entered, summed over n rays (closest hit). Same traversal as
  * pt_trace_closest. counts[5] = {nodes, order, triangles, spheres, instances}. */
 pt_status pt_trace_count(pt_scene* scene, const float* rays, size_t n, float tmin, float tmax, uint64_t counts[5]);
+
+/* ---- triangles (host) ------------------------------------------------------ */
+/* The reference's triangle constructors (include/triangle.hpp:26-35): e1, e2
+ * and the face normal from the corners p0, p1, p2 in its float arithmetic;
+ * normals (9 floats: n0, n1, n2) or, when null, the face normal at every
+ * vertex (the flat constructor); texture coordinates zero. */
+pt_status pt_triangle_init(const float p0[3], const float p1[3], const float p2[3], const float* normals,
+                           uint32_t material, pt_triangle* out);
 
 /* ---- instance transforms (host) -------------------------------------------- */
 /* affine::inverse (include/transform.hpp:42-59): cofactors and determinant in

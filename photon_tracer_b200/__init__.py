@@ -8,8 +8,8 @@ or without an sm_100 GPU, calls raise.
 from . import abi
 from .abi import PhotonError, load
 from .api import (Batch, Generated, Scene, SceneInfo, affine_inverse, batch_scenes, bvh_build, camera_look_at,
-                  denoise_atrous, generate_rays, render_row_linear, write_image)
+                  denoise_atrous, generate_rays, render_row_linear, triangle, write_image)
 
 __all__ = ["abi", "load", "PhotonError", "Batch", "affine_inverse", "batch_scenes", "Generated", "Scene", "SceneInfo",
            "bvh_build", "camera_look_at",
-           "denoise_atrous", "generate_rays", "render_row_linear", "write_image"]
+           "denoise_atrous", "generate_rays", "render_row_linear", "triangle", "write_image"]

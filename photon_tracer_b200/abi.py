@@ -170,6 +170,8 @@ PROTOTYPES = [
     ("pt_primary_depth_device", ST, [P, C.POINTER(pt_camera), C.c_int, C.c_int, P, P]),
     ("pt_trace_count", ST, [P, P, SIZE, C.c_float, C.c_float, C.POINTER(C.c_uint64)]),
     ("pt_affine_inverse", ST, [C.POINTER(pt_affine), C.POINTER(pt_affine)]),
+    ("pt_triangle_init", ST, [C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(C.c_float),
+                              C.c_uint32, C.POINTER(pt_triangle)]),
     ("pt_bvh_build", ST, [P, C.c_uint32, C.POINTER(C.POINTER(pt_bvh_node)), C.POINTER(C.c_uint32),
                           C.POINTER(C.POINTER(C.c_uint32))]),
     ("pt_bvh_build_gpu", ST, [P, C.c_uint32, C.POINTER(C.POINTER(pt_bvh_node)), C.POINTER(C.c_uint32),

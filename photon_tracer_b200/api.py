@@ -67,6 +67,20 @@ def generate_rays(seed: int, lo, hi, n: int) -> np.ndarray:
 
 
 # ---- BVH --------------------------------------------------------------------------
+def triangle(p0, p1, p2, normals=None, material: int = 0, uv=None) -> "abi.pt_triangle":
+    """A pt_triangle as the reference's constructors make it from its corners
+    (e1, e2, face normal derived; normals = three vertex normals or None for a
+    flat triangle); uv: six texture coordinates or None."""
+    fl = lambda v, n: (C.c_float * n)(*[float(x) for x in np.asarray(v, np.float32).reshape(-1)])
+    out = abi.pt_triangle()
+    nrm = fl(normals, 9) if normals is not None else None
+    check(load().pt_triangle_init(fl(p0, 3), fl(p1, 3), fl(p2, 3), nrm, int(material), C.byref(out)))
+    if uv is not None:
+        for k, x in enumerate(np.asarray(uv, np.float32).reshape(6)):
+            out.uv[k] = float(x)
+    return out
+
+
 def affine_inverse(to_world: "abi.pt_affine") -> "abi.pt_affine":
     """The to_object an instance must carry for to_world (affine::inverse)."""
     out = abi.pt_affine()

@@ -190,6 +190,16 @@ const char* pt_version(void) { return "photon_cuda 0.1 (sm_100a)"; }
 
 void pt_free(void* p) { std::free(p); }
 
+pt_status pt_triangle_init(const float p0[3], const float p1[3], const float p2[3], const float* normals,
+                           uint32_t material, pt_triangle* out) {
+    clear_error();
+    if (!p0 || !p1 || !p2 || !out) return fail(PT_ERR_INVALID_ARG, "pt_triangle_init: null pointer");
+    *out = normals ? make_triangle(load(p0), load(p1), load(p2), load(normals), load(normals + 3), load(normals + 6),
+                                   material)
+                   : make_triangle(load(p0), load(p1), load(p2), material);
+    return PT_OK;
+}
+
 pt_status pt_affine_inverse(const pt_affine* to_world, pt_affine* to_object) {
     clear_error();
     if (!to_world || !to_object) return fail(PT_ERR_INVALID_ARG, "pt_affine_inverse: null pointer");

@@ -159,6 +159,28 @@ def test_oracle_random_materials_match_reference(built):
         assert io.tobytes() == ir.tobytes() and ao.tobytes() == ar.tobytes() and ro == rr, seed
 
 
+def test_triangle_init_matches_reference(built):
+    """pt_triangle_init derives e1, e2 and the face normal from the corners
+    bit for bit as the reference's triangle constructor does, over corners
+    from 1e-3 to 1e3 in scale."""
+    import ctypes as C
+    from handmade import scene_from
+    from oracle.oracle import Reference, ref_available
+    from photon_tracer_b200 import abi
+    if not ref_available():
+        pytest.skip("reference harness absent")
+    rng = np.random.default_rng(1)
+    tris = [built.triangle(*(rng.normal(0, 10 ** rng.uniform(-3, 3), 3) for _ in range(3))) for _ in range(500)]
+    d = scene_from(built, [abi.pt_material(type=0, albedo=abi.F3(0.5, 0.5, 0.5))], (), tris)
+    r = Reference(d.desc)
+    out = (C.c_float * 12)()
+    for i, t in enumerate(tris):
+        r.lib.ref_triangle_fields(r.h, -1, i, out)
+        mine = np.array([list(t.p0), list(t.e1), list(t.e2), list(t.face_normal)], np.float32)
+        assert mine.tobytes() == np.array(out[:], np.float32).tobytes(), i
+        assert list(t.n0) == list(t.face_normal) == list(t.n2)
+
+
 def test_instance_transforms_match_reference(built):
     """pt_affine_inverse gives the reference's affine::inverse bit for bit
     (singular matrices included: infinities and NaN alike), and with it the

@@ -187,3 +187,24 @@ def random_transform_instances(pt, seed, singular=False):
             inst.to_world.t[r] = float(t[r])
         inst.to_object = pt.affine_inverse(inst.to_world)
     return g
+
+
+def light_and_radius_scene(pt, seed):
+    """Many emissive spheres (some overlapping, tiny or huge), spheres of
+    radius 0, -0, 1e-30, 1e-7, +-0.5 and 1e15 over all four material kinds,
+    two large spheres of 1e2..1e5 radius, and a camera: (description, camera)."""
+    from photon_tracer_b200 import abi
+    rng = np.random.default_rng(seed)
+    mats = [abi.pt_material(type=0, albedo=abi.F3(*rng.uniform(0, 1, 3).tolist())),
+            abi.pt_material(type=3, emission=abi.F3(*rng.uniform(0.5, 8, 3).tolist())),
+            abi.pt_material(type=1, albedo=abi.F3(0.8, 0.8, 0.8), fuzz=0.2),
+            abi.pt_material(type=2, ior=1.5)]
+    sph = [abi.pt_sphere(center=abi.F3(*rng.uniform(-3, 3, 3).tolist()), radius=float(rng.uniform(0.05, 1.5)),
+                         material=1) for _ in range(int(rng.integers(1, 12)))]
+    radii = [0.0, -0.0, 1e-30, 1e-7, 0.5, -0.5, 1e15, 1.0]
+    sph += [abi.pt_sphere(center=abi.F3(*rng.uniform(-3, 3, 3).tolist()), radius=float(rng.choice(radii)),
+                          material=int(rng.integers(4))) for _ in range(15)]
+    large = [abi.pt_sphere(center=abi.F3(*(rng.uniform(-1, 1, 3) * 10 ** rng.uniform(2, 5)).tolist()),
+                           radius=float(10 ** rng.uniform(2, 5)), material=int(rng.choice([0, 2]))) for _ in range(2)]
+    cam = pt.camera_look_at(tuple(rng.uniform(-6, 6, 3).tolist()), (0.0, 0.0, 0.0), float(rng.uniform(20, 90)), 1.5)
+    return scene_from(pt, mats, sph, (), large), cam

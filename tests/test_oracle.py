@@ -159,6 +159,24 @@ def test_oracle_random_materials_match_reference(built):
         assert io.tobytes() == ir.tobytes() and ao.tobytes() == ar.tobytes() and ro == rr, seed
 
 
+def test_oracle_lights_and_sphere_radii_match_reference(built):
+    """Next-event estimation over many (overlapping, tiny, huge) lights, and
+    spheres of zero, negative-zero, denormal-scale and huge radius: oracle
+    hits and renders equal the reference's."""
+    from handmade import light_and_radius_scene
+    from oracle.oracle import Oracle, Reference, ref_available
+    if not ref_available():
+        pytest.skip("reference harness absent")
+    for seed in range(6):
+        d, cam = light_and_radius_scene(built, 2100 + seed)
+        o, r = Oracle(d.desc), Reference(d.desc)
+        rays = built.generate_rays(seed, [-5, -5, -5], [5, 5, 5], 4000)
+        assert o.trace_closest(rays).tobytes() == r.trace_closest(rays)[0].tobytes()
+        io, ao, ro = o.render(cam, 24, 16, 4, 10, seed=seed, rng_mode=2, aux=True)
+        ir, ar, rr = r.render(cam, 24, 16, 4, 10, seed=seed, aux=True)
+        assert io.tobytes() == ir.tobytes() and ao.tobytes() == ar.tobytes() and ro == rr, seed
+
+
 def test_triangle_init_matches_reference(built):
     """pt_triangle_init derives e1, e2 and the face normal from the corners
     bit for bit as the reference's triangle constructor does, over corners

@@ -20,9 +20,9 @@ namespace {
 constexpr int kTileW = 8, kTileH = 4;
 
 // Resident 128-thread blocks per SM the register allocation targets (5: at
-// most 96 registers; with the flat-scene form's 58 bytes of spills, +6.6% on
-// the 1024x1024 room frame and +8% on the 10,000-instance frame against 3 and
-// 4, which the compiler met with 116-128 registers; 6 lost).
+// most 96 registers; +6.6% on the 1024x1024 room frame and +8% on the
+// 10,000-instance frame against 3 and 4, which the compiler met with 116-128
+// registers; 6 lost).
 #ifndef PT_MEGA_MIN_BLOCKS
 #define PT_MEGA_MIN_BLOCKS 5
 #endif
@@ -30,15 +30,16 @@ constexpr int kTileW = 8, kTileH = 4;
 // The pixel coordinates, sample number and running sum of each lane in
 // shared memory instead of registers (they change once per path): 170 -> 100
 // bytes of spills in the flat-scene form, room frame +0.8%, images identical.
-// The path state of each lane in shared memory in the flat-scene form: no
-// spills left there, room frame +1.0%, random spheres +3.7%; the instanced
+#ifndef PT_MEGA_SMEM_STATE
+#define PT_MEGA_SMEM_STATE 1
+#endif
+
+// The path state of each lane in shared memory too, in the flat-scene form:
+// no spills left there, room frame +1.0%, random spheres +3.7%; the instanced
 // form lost 3% with it and keeps registers (the RNG state moved as well
 // gained nothing more).
 #ifndef PT_MEGA_SMEM_PATH
 #define PT_MEGA_SMEM_PATH 1
-#endif
-#ifndef PT_MEGA_SMEM_STATE
-#define PT_MEGA_SMEM_STATE 1
 #endif
 
 // Scenes without instances trace one query per loop trip (a path ray or a

@@ -177,6 +177,22 @@ def test_oracle_lights_and_sphere_radii_match_reference(built):
         assert io.tobytes() == ir.tobytes() and ao.tobytes() == ar.tobytes() and ro == rr, seed
 
 
+def test_camera_matches_reference_including_degenerate(built):
+    """pt_camera_look_at at 16:9 against the reference's camera constructor:
+    random placements and fields of view, and degenerate ones (eye at the
+    target, looking straight up or down, fov 0 and 179.9, eye at 1e30)."""
+    from oracle.oracle import ref_available, ref_camera
+    if not ref_available():
+        pytest.skip("reference harness absent")
+    rng = np.random.default_rng(4)
+    cases = [((0, 0, 0), (0, 0, 0), 40.0), ((0, 5, 0), (0, 0, 0), 40.0), ((0, -5, 0), (0, 0, 0), 40.0),
+             ((1, 2, 3), (1, 2, 3.0001), 1e-3), ((1, 2, 3), (4, 5, 6), 179.9), ((1, 2, 3), (4, 5, 6), 0.0),
+             ((1e30, 0, 0), (0, 0, 0), 40.0), ((0, 0, 1e-30), (0, 0, 0), 40.0)]
+    cases += [(tuple(rng.normal(0, 10, 3)), tuple(rng.normal(0, 1, 3)), float(rng.uniform(1, 170))) for _ in range(200)]
+    for lf, la, v in cases:
+        assert bytes(memoryview(built.camera_look_at(lf, la, v))) == bytes(memoryview(ref_camera(lf, la, v))), (lf, la, v)
+
+
 def test_triangle_init_matches_reference(built):
     """pt_triangle_init derives e1, e2 and the face normal from the corners
     bit for bit as the reference's triangle constructor does, over corners

@@ -60,7 +60,7 @@ struct Scratch {
 };
 
 struct pt_scene {
-    PtSceneDev dev;
+    PtSceneDev dev{};
     pt_scene_info info;
     int device = 0;
     int sms = 148;

@@ -40,7 +40,7 @@ struct pt_batch {
     int device = 0, sms = 148;
     void* arena = nullptr;
     size_t arena_bytes = 0;
-    PtSceneDev dev;
+    PtSceneDev dev{};
     std::vector<PtBatchScene> scenes;
     std::vector<pt_batch_item> items;
     PtBatchScene* d_scenes = nullptr;

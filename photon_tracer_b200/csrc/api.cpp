@@ -236,14 +236,16 @@ pt_status pt_scene_create(const pt_scene_desc* desc, pt_scene** out) {
     clear_error();
     if (!desc || !out) return fail(PT_ERR_INVALID_ARG, "pt_scene_create: null pointer");
     *out = nullptr;
-    int device = 0, sms = 0;
-    if (pt_status st = check_device(device, sms)) return st;
+    // The description is checked and packed on the host first, so that its
+    // errors are reported the same with or without a device.
     HostArena A;
     try {
         if (pt_status st = build_arena(*desc, A)) return st;
     } catch (const std::bad_alloc&) {
         return fail(PT_ERR_OUT_OF_MEMORY, "pt_scene_create: out of host memory");
     }
+    int device = 0, sms = 0;
+    if (pt_status st = check_device(device, sms)) return st;
     pt_scene* s = new (std::nothrow) pt_scene();
     if (!s) return fail(PT_ERR_OUT_OF_MEMORY, "pt_scene_create: out of host memory");
     s->device = device;

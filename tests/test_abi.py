@@ -83,17 +83,57 @@ def test_invalid_arguments_return_codes(built):
 
 
 def test_scene_validation_before_device(built):
-    """Descriptions with out-of-range references are refused by the repack,
-    which runs on the host (no device needed to see the error code, except
-    that without a device the device check answers first)."""
+    """Invalid descriptions are refused by the host-side repack, before any
+    device is touched, with PT_ERR_INVALID_ARG and a message naming the
+    field (so the same answer comes with or without a GPU)."""
     from photon_tracer_b200 import abi
     lib = built.load()
-    mats = (abi.pt_material * 1)(abi.pt_material(type=0, albedo=abi.F3(0.5, 0.5, 0.5)))
-    sph = (abi.pt_sphere * 1)(abi.pt_sphere(center=abi.F3(0, 0, 0), radius=1.0, material=7))
-    d = abi.pt_scene_desc(materials=mats, n_materials=1, spheres=sph, n_spheres=1, use_bvh=1, sky=1)
-    h = C.c_void_p()
-    st = lib.pt_scene_create(C.byref(d), C.byref(h))
-    assert st in (abi.PT_ERR_INVALID_ARG, abi.PT_ERR_NO_DEVICE)
+    mat = abi.pt_material(type=0, albedo=abi.F3(0.5, 0.5, 0.5))
+    px = (C.c_uint8 * 3)(1, 2, 3)
+
+    def create(**kw):
+        keep = []
+
+        def arr(t, items):
+            a = (t * max(1, len(items)))(*items)
+            keep.append(a)
+            return a
+        mats = kw.pop("materials", [mat])
+        sph = kw.pop("spheres", [])
+        tris = kw.pop("triangles", [])
+        meshes = kw.pop("meshes", [])
+        inst = kw.pop("instances", [])
+        tex = kw.pop("textures", [])
+        lights = kw.pop("lights", None)
+        d = abi.pt_scene_desc(materials=arr(abi.pt_material, mats), n_materials=len(mats),
+                              spheres=arr(abi.pt_sphere, sph), n_spheres=len(sph),
+                              triangles=arr(abi.pt_triangle, tris), n_triangles=len(tris),
+                              meshes=arr(abi.pt_mesh, meshes), n_meshes=len(meshes),
+                              instances=arr(abi.pt_instance, inst), n_instances=len(inst),
+                              textures=arr(abi.pt_texture, tex), n_textures=len(tex), use_bvh=1, sky=1)
+        if lights is not None:
+            d.lights = arr(C.c_uint32, lights)
+            d.n_lights = len(lights)
+        h = C.c_void_p()
+        st = lib.pt_scene_create(C.byref(d), C.byref(h))
+        return st, lib.pt_last_error().decode()
+
+    tri = built.triangle((0, 0, 0), (1, 0, 0), (0, 1, 0), material=3)
+    mesh_tri = (abi.pt_triangle * 1)(built.triangle((0, 0, 0), (1, 0, 0), (0, 1, 0)))
+    mesh = abi.pt_mesh(triangles=mesh_tri, n_triangles=1)
+    cases = [
+        (dict(spheres=[abi.pt_sphere(radius=1.0, material=7)]), "sphere: material"),
+        (dict(triangles=[tri]), "triangle: material"),
+        (dict(materials=[abi.pt_material(type=9)]), "unknown type"),
+        (dict(materials=[abi.pt_material(type=0, texture=2)], textures=[abi.pt_texture(1, 1, px)]), "texture out"),
+        (dict(textures=[abi.pt_texture(0, 4, px)]), "texture: empty"),
+        (dict(meshes=[mesh], instances=[abi.pt_instance(mesh=3)]), "instance: mesh"),
+        (dict(meshes=[mesh], instances=[abi.pt_instance(mesh=0, material=5)]), "instance: material"),
+        (dict(spheres=[abi.pt_sphere(radius=1.0)], lights=[4]), "light: sphere"),
+    ]
+    for kw, words in cases:
+        st, msg = create(**kw)
+        assert st == abi.PT_ERR_INVALID_ARG and words in msg, (words, st, msg)
 
 
 def test_no_device_is_an_error_not_a_fallback(built):

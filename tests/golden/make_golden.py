@@ -13,7 +13,10 @@ reference:
 * ref_render_*.npz    -- small renders by the reference's own per-row stream,
   with the xoshiro state captured before every sample's path;
 * ref_trees.json      -- digests of the trees the reference's geometry::build
-  makes for every scene generator.
+  makes for every scene generator;
+* ref_denoise.npz     -- the reference's a-trous denoise of a small render of
+  its own (colour, albedo, normal, per-pixel luminance variance) and of
+  seeded random planes.
 
     python tests/golden/make_golden.py
 """
@@ -66,6 +69,24 @@ def tree_digest(trees) -> list:
     return out
 
 
+def write_denoise():
+    from oracle.oracle import ref_denoise
+    g = pt.Generated(abi.PT_GEN_ROOM_MESH, seed=1, param=3)
+    r = Reference(g.desc)
+    img, aux, _ = r.render(g.camera, 48, 32, 4, 10, seed=5, aux=True)
+    lum = 0.2126 * img[..., 0] + 0.7152 * img[..., 1] + 0.0722 * img[..., 2]
+    cases = {"render": (img, aux[..., 0:3], aux[..., 3:6], np.maximum(aux[..., 6] - lum * lum, 0))}
+    rng = np.random.default_rng(7)
+    cases["random"] = (rng.random((32, 45, 3), dtype=np.float32) * 3, rng.random((32, 45, 3), dtype=np.float32),
+                       rng.normal(size=(32, 45, 3)).astype(np.float32), rng.random((32, 45), dtype=np.float32))
+    arrays = {}
+    for name, (c, al, nrm, var) in cases.items():
+        c, al, nrm, var = (np.ascontiguousarray(x, np.float32) for x in (c, al, nrm, var))
+        arrays.update({f"{name}_color": c, f"{name}_albedo": al, f"{name}_normal": nrm, f"{name}_variance": var,
+                       f"{name}_out": ref_denoise(c, al, nrm, var)})
+    np.savez_compressed(os.path.join(HERE, "ref_denoise.npz"), **arrays)
+
+
 def main():
     ref_json = os.path.join(REFERENCE, "tests", "reference.json")
     with open(ref_json) as f:
@@ -107,6 +128,7 @@ def main():
         digests[name] = {"kind": kind, "param": param, "trees": tree_digest(reference_trees(r, g.desc))}
     with open(os.path.join(HERE, "ref_trees.json"), "w") as f:
         json.dump(digests, f, indent=1)
+    write_denoise()
     print("wrote fixtures to", HERE)
 
 

@@ -244,6 +244,23 @@ def test_instance_transforms_match_reference(built):
     assert io.tobytes() == ir.tobytes() and ao.tobytes() == ar.tobytes() and ro == rr
 
 
+def test_oracle_denoise_matches_reference(built):
+    """The oracle's a-trous filter against the reference's denoise: bit for
+    bit on the committed fixture (a render of the reference's and random
+    planes), and live on other random inputs when the reference is built."""
+    from oracle.oracle import oracle_denoise, ref_available, ref_denoise
+    f = golden("ref_denoise.npz")
+    for name in ("render", "random"):
+        got = oracle_denoise(f[f"{name}_color"], f[f"{name}_albedo"], f[f"{name}_normal"], f[f"{name}_variance"])
+        assert got.tobytes() == f[f"{name}_out"].tobytes(), name
+    if ref_available():
+        rng = np.random.default_rng(3)
+        for h, w in ((17, 29), (64, 5)):
+            c, al = rng.random((h, w, 3), dtype=np.float32) * 4, rng.random((h, w, 3), dtype=np.float32)
+            nrm, var = rng.normal(size=(h, w, 3)).astype(np.float32), rng.random((h, w), dtype=np.float32)
+            assert oracle_denoise(c, al, nrm, var).tobytes() == ref_denoise(c, al, nrm, var).tobytes()
+
+
 def test_sampler_known_answers(built):
     """The Sobol pairs (sampler.hpp) of the oracle against the reference's, and
     the superset-XOR form of the second Sobol dimension the GPU computes."""

@@ -16,7 +16,10 @@ reference:
   makes for every scene generator;
 * ref_denoise.npz     -- the reference's a-trous denoise of a small render of
   its own (colour, albedo, normal, per-pixel luminance variance) and of
-  seeded random planes.
+  seeded random planes;
+* ref_edge_hits.npz   -- the reference's closest/any hits for rays with
+  infinite, signed-zero, denormal and huge components (room scene), and on
+  the hand-made scenes with NaN and huge coordinates (tests/handmade.py).
 
     python tests/golden/make_golden.py
 """
@@ -87,6 +90,26 @@ def write_denoise():
     np.savez_compressed(os.path.join(HERE, "ref_denoise.npz"), **arrays)
 
 
+def write_edge_hits():
+    sys.path.insert(0, os.path.dirname(HERE))
+    from handmade import adversarial_rays, non_finite_scene, non_finite_spheres
+    arrays = {}
+    g = pt.Generated(abi.PT_GEN_ROOM_MESH, seed=2, param=3)
+    r = Reference(g.desc)
+    rays = adversarial_rays(9, 20000)[:5000]
+    hits, _ = r.trace_closest(rays)
+    arrays.update(adversarial_rays=rays, adversarial_hits=hits.view(np.uint32).reshape(-1, 6),
+                  adversarial_occluded=r.trace_any(rays))
+    for name, make in (("nan_triangles", non_finite_scene), ("nan_spheres", non_finite_spheres)):
+        d, rays = make(pt)
+        rays = rays[:5000]
+        r = Reference(d.desc)
+        hits, _ = r.trace_closest(rays)
+        arrays.update({f"{name}_rays": rays, f"{name}_hits": hits.view(np.uint32).reshape(-1, 6),
+                       f"{name}_occluded": r.trace_any(rays)})
+    np.savez_compressed(os.path.join(HERE, "ref_edge_hits.npz"), **arrays)
+
+
 def main():
     ref_json = os.path.join(REFERENCE, "tests", "reference.json")
     with open(ref_json) as f:
@@ -129,6 +152,7 @@ def main():
     with open(os.path.join(HERE, "ref_trees.json"), "w") as f:
         json.dump(digests, f, indent=1)
     write_denoise()
+    write_edge_hits()
     print("wrote fixtures to", HERE)
 
 

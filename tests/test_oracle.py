@@ -244,6 +244,24 @@ def test_instance_transforms_match_reference(built):
     assert io.tobytes() == ir.tobytes() and ao.tobytes() == ar.tobytes() and ro == rr
 
 
+def test_oracle_edge_hits_match_reference_fixture(built):
+    """Closest and any hits the reference made for adversarial rays (room
+    scene) and on the NaN-geometry scenes, pinned as a fixture: the oracle
+    reproduces them without the reference present."""
+    from handmade import non_finite_scene, non_finite_spheres
+    from oracle.oracle import Oracle
+    from photon_tracer_b200 import abi
+    f = golden("ref_edge_hits.npz")
+    g = built.Generated(abi.PT_GEN_ROOM_MESH, seed=2, param=3)
+    scenes = [("adversarial", g.desc), ("nan_triangles", non_finite_scene(built)[0].desc),
+              ("nan_spheres", non_finite_spheres(built)[0].desc)]
+    for name, desc in scenes:
+        o = Oracle(desc)
+        rays = f[f"{name}_rays"]
+        assert o.trace_closest(rays).view(np.uint32).reshape(-1, 6).tobytes() == f[f"{name}_hits"].tobytes(), name
+        assert np.array_equal(o.trace_any(rays), f[f"{name}_occluded"]), name
+
+
 def test_oracle_denoise_matches_reference(built):
     """The oracle's a-trous filter against the reference's denoise: bit for
     bit on the committed fixture (a render of the reference's and random

@@ -19,7 +19,10 @@ reference:
   seeded random planes;
 * ref_edge_hits.npz   -- the reference's closest/any hits for rays with
   infinite, signed-zero, denormal and huge components (room scene), and on
-  the hand-made scenes with NaN and huge coordinates (tests/handmade.py).
+  the hand-made scenes with NaN and huge coordinates (tests/handmade.py);
+* ref_material_renders.npz -- the reference's renders (24x16, 4 spp, image,
+  guides, ray count) of four random-material scenes (tests/handmade.py:
+  metal fuzz above 1, ior at and below 1, negative radii, emitters).
 
     python tests/golden/make_golden.py
 """
@@ -110,6 +113,17 @@ def write_edge_hits():
     np.savez_compressed(os.path.join(HERE, "ref_edge_hits.npz"), **arrays)
 
 
+def write_material_renders():
+    sys.path.insert(0, os.path.dirname(HERE))
+    from handmade import random_material_scene
+    arrays = {}
+    for seed in range(4):
+        d, cam = random_material_scene(pt, 500 + seed)
+        img, aux, rays = Reference(d.desc).render(cam, 24, 16, 4, 10, seed=seed, aux=True)
+        arrays.update({f"s{seed}_image": img, f"s{seed}_aux": aux, f"s{seed}_rays": np.uint64(rays)})
+    np.savez_compressed(os.path.join(HERE, "ref_material_renders.npz"), **arrays)
+
+
 def main():
     ref_json = os.path.join(REFERENCE, "tests", "reference.json")
     with open(ref_json) as f:
@@ -153,6 +167,7 @@ def main():
         json.dump(digests, f, indent=1)
     write_denoise()
     write_edge_hits()
+    write_material_renders()
     print("wrote fixtures to", HERE)
 
 

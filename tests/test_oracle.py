@@ -142,6 +142,20 @@ def test_oracle_adversarial_rays_match_reference(built):
             assert np.array_equal(o.trace_any(rays), r.trace_any(rays))
 
 
+def test_oracle_material_renders_match_reference_fixture(built):
+    """Renders the reference made of four random-material scenes (metal fuzz
+    above 1 among them), pinned as a fixture: the oracle reproduces image,
+    guides and ray count without the reference present."""
+    from handmade import random_material_scene
+    from oracle.oracle import Oracle
+    f = golden("ref_material_renders.npz")
+    for seed in range(4):
+        d, cam = random_material_scene(built, 500 + seed)
+        img, aux, rays = Oracle(d.desc).render(cam, 24, 16, 4, 10, seed=seed, rng_mode=2, aux=True)
+        assert img.tobytes() == f[f"s{seed}_image"].tobytes() and aux.tobytes() == f[f"s{seed}_aux"].tobytes()
+        assert rays == int(f[f"s{seed}_rays"])
+
+
 def test_oracle_random_materials_match_reference(built):
     """Random scenes over all four material kinds and their edge parameters
     (metal fuzz above 1, dielectric ior at and below 1, negative radii,

@@ -79,6 +79,29 @@ def test_oracle_no_bvh_matches_reference(built):
     assert o.trace_closest(rays).tobytes() == r.trace_closest(rays)[0].tobytes()
 
 
+def test_oracle_random_render_settings_match_reference(built):
+    """Renders through the reference's per-row stream over random settings:
+    frame sizes down to 1x1, depth 0 to 11, 1 to 5 spp, sample offsets, five
+    scene families."""
+    from oracle.oracle import Oracle, Reference, ref_available
+    if not ref_available():
+        pytest.skip("reference harness absent")
+    from photon_tracer_b200 import abi
+    rng = np.random.default_rng(11)
+    scenes = [(abi.PT_GEN_ROOM_MESH, 3), (abi.PT_GEN_REF_MATERIALS, 0), (abi.PT_GEN_INSTANCES, 40),
+              (abi.PT_GEN_RANDOM_SPHERES, 0), (abi.PT_GEN_TEXTURED, 0)]
+    for trial in range(15):
+        kind, param = scenes[trial % len(scenes)]
+        g = built.Generated(kind, seed=int(rng.integers(1, 50)), param=param)
+        w, h = int(rng.integers(1, 20)), int(rng.integers(1, 14))
+        spp, depth = int(rng.integers(1, 6)), int(rng.integers(0, 12))
+        seed, fs = int(rng.integers(0, 1 << 30)), int(rng.integers(0, 100))
+        io, ao, ro = Oracle(g.desc).render(g.camera, w, h, spp, depth, seed=seed, rng_mode=2, aux=True,
+                                           first_sample=fs)
+        ir, ar, rr = Reference(g.desc).render(g.camera, w, h, spp, depth, seed=seed, aux=True, first_sample=fs)
+        assert io.tobytes() == ir.tobytes() and ao.tobytes() == ar.tobytes() and ro == rr, (kind, w, h, spp, depth)
+
+
 def test_oracle_non_finite_geometry_matches_reference(built):
     """NaN and huge coordinates in triangles (flat and instanced) and
     spheres: the oracle builds the reference's trees (std::min / std::max

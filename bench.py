@@ -431,6 +431,21 @@ def run_scene_workload(args, kind, label, param=0):
     return 0
 
 
+def over_ranks(dist, device, ms_total, rays, e2e_ms, rays_e2e):
+    """Whole-job figures over the ranks of a replicated run: the slowest
+    rank's timed and end-to-end times, and the rays of all ranks, as
+    (ms_total, rays, e2e_ms, rays_e2e). dist is torch.distributed with an
+    initialised group, or None for one process."""
+    if dist is None:
+        return ms_total, rays, e2e_ms, rays_e2e
+    import torch
+    t = torch.tensor([ms_total, e2e_ms], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    r = torch.tensor([rays, rays_e2e], dtype=torch.int64, device=device)
+    dist.all_reduce(r, op=dist.ReduceOp.SUM)
+    return float(t[0].item()), int(r[0].item()), float(t[1].item()), int(r[1].item())
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
     ap.add_argument("--gpus", type=int, default=1)
@@ -528,27 +543,22 @@ def main():
     times = [s.elapsed_time(e) for s, e in zip(starts, ends)]
     ms_total = float(sum(times))
     rays_total = int(rays_dev.item())
-    if world > 1:
-        t = torch.tensor([ms_total], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        r = torch.tensor([rays_total], dtype=torch.int64, device="cuda")
-        dist.all_reduce(r, op=dist.ReduceOp.SUM)
-        ms_total, rays_all = float(t.item()), int(r.item())
-    else:
-        rays_all = rays_total
-    value = rays_all / (ms_total / 1e3) / 1e6
-    rays_per_launch = rays_total / args.steps
-    ms_per_launch = ms_total / args.steps
 
     # End to end through the public host-buffer call: camera and settings in,
     # the frame (and ray count) back to host memory, every step.
     e2e_ms = []
     img = None
+    rays_e2e = 0
     for k in range(max(2, min(args.steps, 5))):
         t0 = time.perf_counter()
         img, _, rays_e2e = scene.render(g.camera, WIDTH, HEIGHT, SPP, DEPTH, seed=SEED, mode=mode)
         e2e_ms.append((time.perf_counter() - t0) * 1e3)
-    e2e_value = rays_e2e / (statistics.mean(e2e_ms) / 1e3) / 1e6 * world
+    ms_total, rays_all, e2e_ms_slowest, rays_e2e_all = over_ranks(
+        dist if world > 1 else None, "cuda", ms_total, rays_total, statistics.mean(e2e_ms), int(rays_e2e))
+    value = rays_all / (ms_total / 1e3) / 1e6
+    rays_per_launch = rays_total / args.steps
+    ms_per_launch = ms_total / args.steps
+    e2e_value = rays_e2e_all / (e2e_ms_slowest / 1e3) / 1e6
 
     line = None
     if rank == 0:
@@ -581,7 +591,7 @@ def main():
             "e2e": {"value": round(e2e_value, 2), "unit": "Mrays/s",
                     "h2d_bytes_per_step": C.sizeof(abi.pt_camera) + C.sizeof(abi.pt_settings),
                     "d2h_bytes_per_step": int(img.nbytes) + 8, "api": "pt_render (host buffers)",
-                    "ms_per_step": round(statistics.mean(e2e_ms), 3)},
+                    "ms_per_step": round(e2e_ms_slowest, 3)},
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 4), "traffic": traffic, "peak_kind": peak_kind,
                          "bytes_per_ray": round(bpr, 2), "kernel": "megakernel",

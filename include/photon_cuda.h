@@ -354,8 +354,9 @@ size_t pt_denoise_atrous_scratch_floats(int width, int height);
  * takes its scratch from a fixed array inside the library, which every GPU
  * that loads the library holds (11.5 MB) until the process exits. Frames of
  * more than PT_ATROUS_NOALLOC_MAX_PIXELS pixels are refused with
- * PT_ERR_INVALID_ARG. The first call on each device looks up the array's
- * device address (make it before any stream capture). All calls share the
+ * PT_ERR_INVALID_ARG. The first call in each CUDA context looks up the
+ * array's device address (make the first call on a device, and the first after
+ * a cudaDeviceReset, before any stream capture). All calls share the
  * array: calls whose work overlaps on the GPU (other streams, other threads)
  * race and corrupt each other's output. Device buffers, enqueued on stream. */
 #define PT_ATROUS_NOALLOC_MAX_PIXELS 262144

@@ -43,6 +43,8 @@ PT_GEN_INSTANCES = 12
 PT_GEN_BATCH_SCENE = 13
 PT_GEN_TEXTURED = 14
 
+PT_ATROUS_NOALLOC_MAX_PIXELS = 262144  # the built-in scratch of pt_denoise_atrous_device_noalloc
+
 F3 = C.c_float * 3
 
 

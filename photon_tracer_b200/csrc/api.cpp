@@ -100,7 +100,9 @@ pt_status read_status(pt_scene* s, cudaStream_t stream) {
     unsigned int st = 0;
     if (cudaError_t e = cudaMemcpy(&st, s->status, sizeof(st), cudaMemcpyDeviceToHost)) return cuda_fail(e, "status");
     if (st) {
-        cudaMemset(s->status, 0, sizeof(unsigned int));
+        // Cleared on the scene's stream, so the clear is ordered before the
+        // next kernel that may set a bit again.
+        cudaMemsetAsync(s->status, 0, sizeof(unsigned int), stream);
         if (st & PT_DEV_ERR_STACK) return fail(PT_ERR_STACK_OVERFLOW, "a traversal stack overflowed on the device");
         if (st & PT_DEV_ERR_QUEUE) return fail(PT_ERR_QUEUE_OVERFLOW, "a wavefront queue overflowed on the device");
         if (st & PT_DEV_ERR_TIMEOUT) return fail(PT_ERR_TIMEOUT, "a device wait timed out");

@@ -62,6 +62,7 @@ struct pt_batch {
     double tune_ms[5] = {0, 0, 0, 0, 0};
     std::vector<cudaEvent_t> scene_events;  // per-scene completion (per-scene strategies)
     cudaEvent_t start_event = nullptr;
+    cudaEvent_t done_event = nullptr;  // recorded on the render's stream after its last launch
     int last_strategy = 0;
 };
 
@@ -258,7 +259,7 @@ double time_ms(pt_batch* b, int strategy, int threads) {
     cudaEventElapsedTime(&ms, a, z);
     cudaEventDestroy(a);
     cudaEventDestroy(z);
-    return st ? 1e30 : double(ms);
+    return st ? -double(st) : double(ms);
 }
 
 std::string shape_key(const pt_batch* b) {
@@ -284,9 +285,21 @@ pt_status tune(pt_batch* b) {
     const Cand cands[5] = {{PT_BATCH_ONE_LAUNCH, 64, 0}, {PT_BATCH_ONE_LAUNCH, 128, 1}, {PT_BATCH_ONE_LAUNCH, 256, 2},
                            {PT_BATCH_PER_SCENE_MEGA, 128, 3}, {PT_BATCH_PER_SCENE_WAVE, 128, 4}};
     double best = 1e30;
+    pt_status first_error = PT_OK;
+    std::string first_message;
+    bool any = false;
     for (const Cand& c : cands) {
-        time_ms(b, c.strategy, c.threads);
-        const double ms = time_ms(b, c.strategy, c.threads);
+        double ms = time_ms(b, c.strategy, c.threads);
+        if (ms >= 0) ms = time_ms(b, c.strategy, c.threads);
+        if (ms < 0) {  // the candidate failed: keep the first failure's status and message
+            if (first_error == PT_OK) {
+                first_error = static_cast<pt_status>(int(-ms));
+                first_message = pt_last_error();
+            }
+            b->tune_ms[c.slot] = 1e30;
+            continue;
+        }
+        any = true;
         b->tune_ms[c.slot] = ms;
         if (ms < best) {
             best = ms;
@@ -294,6 +307,7 @@ pt_status tune(pt_batch* b) {
             b->threads = c.threads;
         }
     }
+    if (!any) return fail(first_error, first_message.c_str());
     b->tuned = true;
     std::lock_guard<std::mutex> lock(g_tune_lock);
     g_tune_cache[shape_key(b)] = {b->strategy, b->threads};
@@ -412,6 +426,7 @@ pt_status pt_batch_create(const pt_batch_item* items, uint32_t n, int32_t strate
     if (!err) err = cudaMemset(base + off, 0, 4 * 256);
     if (!err) err = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
     if (!err) err = cudaEventCreate(&b->start_event);
+    if (!err) err = cudaEventCreateWithFlags(&b->done_event, cudaEventDisableTiming);
     for (uint32_t i = 0; i < n && !err; ++i) {
         cudaEvent_t ev;
         err = cudaEventCreate(&ev);
@@ -444,6 +459,7 @@ pt_status pt_batch_render(pt_batch* b, void* stream_, uint64_t* rays_out) {
     if (cudaError_t e = cudaMemsetAsync(b->d_rays, 0, 8, stream)) return cuda_fail(e, "pt_batch_render");
     const int strategy = b->strategy == PT_BATCH_AUTO ? PT_BATCH_ONE_LAUNCH : b->strategy;
     if (pt_status st = run_strategy(b, strategy, b->threads, stream)) return st;
+    if (cudaError_t e = cudaEventRecord(b->done_event, stream)) return cuda_fail(e, "pt_batch_render");
     if (rays_out) {
         unsigned long long r = 0;
         if (cudaError_t e = cudaMemcpyAsync(&r, b->d_rays, 8, cudaMemcpyDeviceToHost, stream))
@@ -466,10 +482,16 @@ pt_status pt_batch_download(pt_batch* b, uint32_t i, float* host) {
     if (!b || !host || i >= b->scenes.size()) return fail(PT_ERR_INVALID_ARG, "pt_batch_download: bad argument");
     if (cudaError_t e = cudaSetDevice(b->device)) return cuda_fail(e, "cudaSetDevice");
     const size_t floats = 3 * size_t(b->scenes[i].width) * b->scenes[i].height;
-    if (cudaError_t e = cudaMemcpy(host, b->d_out + b->scenes[i].out_offset, floats * 4, cudaMemcpyDeviceToHost))
+    // The last render may have run on a stream the caller passed, which the
+    // copies below are not ordered against: wait for its end first.
+    if (cudaError_t e = cudaEventSynchronize(b->done_event)) return cuda_fail(e, "pt_batch_download");
+    if (cudaError_t e = cudaMemcpyAsync(host, b->d_out + b->scenes[i].out_offset, floats * 4, cudaMemcpyDeviceToHost,
+                                        b->stream))
         return cuda_fail(e, "pt_batch_download");
     unsigned int st = 0;
-    cudaMemcpy(&st, b->d_status, 4, cudaMemcpyDeviceToHost);
+    if (cudaError_t e = cudaMemcpyAsync(&st, b->d_status, 4, cudaMemcpyDeviceToHost, b->stream))
+        return cuda_fail(e, "pt_batch_download: status");
+    if (cudaError_t e = cudaStreamSynchronize(b->stream)) return cuda_fail(e, "pt_batch_download");
     if (st & PT_DEV_ERR_STACK) return fail(PT_ERR_STACK_OVERFLOW, "a traversal stack overflowed on the device");
     return PT_OK;
 }
@@ -479,8 +501,8 @@ pt_status pt_batch_scene_times(pt_batch* b, double* ms) {
     if (!b || !ms) return fail(PT_ERR_INVALID_ARG, "pt_batch_scene_times: null pointer");
     if (cudaError_t e = cudaSetDevice(b->device)) return cuda_fail(e, "cudaSetDevice");
     const size_t n = b->scenes.size();
+    if (cudaError_t e = cudaEventSynchronize(b->done_event)) return cuda_fail(e, "pt_batch_scene_times");
     if (cudaError_t e = cudaStreamSynchronize(b->stream)) return cuda_fail(e, "pt_batch_scene_times");
-    cudaDeviceSynchronize();
     if (b->last_strategy == PT_BATCH_ONE_LAUNCH) {
         std::vector<unsigned long long> done(n);
         unsigned long long start = 0;
@@ -521,6 +543,7 @@ pt_status pt_batch_destroy(pt_batch* b) {
     for (pt_scene* s : b->singles) pt_scene_destroy(s);
     for (cudaEvent_t e : b->scene_events) cudaEventDestroy(e);
     if (b->start_event) cudaEventDestroy(b->start_event);
+    if (b->done_event) cudaEventDestroy(b->done_event);
     if (b->stream) cudaStreamDestroy(b->stream);
     if (b->arena) cudaFree(b->arena);
     delete b;

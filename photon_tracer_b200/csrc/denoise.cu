@@ -168,21 +168,55 @@ pt_status pt_denoise_atrous(int w, int h, const float* color, const float* albed
 // are limited to PT_ATROUS_NOALLOC_MAX_PIXELS pixels.
 //
 // Host code must not hand g_atrous_scratch to a kernel: here its name is only
-// a host-side stand-in. The device address is looked up once per device, with
-// that device current, by the first call on it (cudaGetSymbolAddress), so the
-// first call on each device should come before any stream capture. Every call
+// a host-side stand-in. The device address is looked up once per CUDA context,
+// with that context current, by the first call in it (cudaGetSymbolAddress), so
+// the first call on each device -- and the first after a cudaDeviceReset, which
+// makes a new context where the module may load elsewhere -- should come
+// before any stream capture. Every call
 // uses the same array and leaves the last call's data in it; the filter writes
 // every scratch value before reading it, so nothing needs clearing, but two
 // calls whose work overlaps on the GPU (different streams, or different host
 // threads on one device) race on the array and corrupt each other's output.
 static __device__ __align__(256) float g_atrous_scratch[11 * size_t(PT_ATROUS_NOALLOC_MAX_PIXELS)];
 
+#include <cuda.h>
+
 #include <map>
 #include <mutex>
 
 namespace {
 std::mutex g_scratch_lock;
-std::map<int, float*> g_scratch_addr;  // device ordinal -> device address of g_atrous_scratch
+// CUDA context id -> device address of g_atrous_scratch in that context. Keyed
+// by context, not device ordinal: after a device reset the module is loaded
+// again into a new context (a new id) and its address is looked up again.
+std::map<unsigned long long, float*> g_scratch_addr;
+
+// The id of the calling thread's current context (cuCtxGetId, CUDA 12), or 0
+// when none is current yet. The driver calls are reached through the runtime's
+// entry-point lookup, so the library needs no link against libcuda.
+unsigned long long current_context_id() {
+    using GetCurrent = CUresult (*)(CUcontext*);
+    using GetId = CUresult (*)(CUcontext, unsigned long long*);
+    static GetCurrent get_current = nullptr;
+    static GetId get_id = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_current = reinterpret_cast<GetCurrent>(p);
+        p = nullptr;
+        if (cudaGetDriverEntryPoint("cuCtxGetId", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_id = reinterpret_cast<GetId>(p);
+    });
+    CUcontext ctx = nullptr;
+    unsigned long long id = 0;
+    if (!get_current || !get_id || get_current(&ctx) != CUDA_SUCCESS || !ctx || get_id(ctx, &id) != CUDA_SUCCESS)
+        return 0;
+    return id;
+}
 }  // namespace
 
 extern "C" pt_status pt_denoise_atrous_device_noalloc(int w, int h, const float* color, const float* albedo,
@@ -197,20 +231,23 @@ extern "C" pt_status pt_denoise_atrous_device_noalloc(int w, int h, const float*
                             " pixels its built-in scratch holds; use pt_denoise_atrous_device with your own scratch");
     if (!color || !albedo || !normal || !variance || !out)
         return pt::fail(PT_ERR_INVALID_ARG, "pt_denoise_atrous_device_noalloc: null pointer");
-    int dev = 0;
-    if (pt_status st = cuda_status(cudaGetDevice(&dev), "pt_denoise_atrous_device_noalloc")) return st;
     float* scratch = nullptr;
     {
         std::lock_guard<std::mutex> lock(g_scratch_lock);
-        auto it = g_scratch_addr.find(dev);
+        const unsigned long long ctx = current_context_id();
+        auto it = ctx ? g_scratch_addr.find(ctx) : g_scratch_addr.end();
         if (it == g_scratch_addr.end()) {
+            // Looking the symbol up also makes the device's primary context
+            // current when no runtime call has yet on this thread.
             void* p = nullptr;
             if (pt_status st = cuda_status(cudaGetSymbolAddress(&p, g_atrous_scratch),
                                            "pt_denoise_atrous_device_noalloc: scratch address"))
                 return st;
-            it = g_scratch_addr.emplace(dev, static_cast<float*>(p)).first;
+            scratch = static_cast<float*>(p);
+            if (const unsigned long long now = current_context_id()) g_scratch_addr[now] = scratch;
+        } else {
+            scratch = it->second;
         }
-        scratch = it->second;
     }
     return pt_denoise_atrous_device(w, h, color, albedo, normal, variance, out, scratch, stream);
 }

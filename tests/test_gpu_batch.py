@@ -66,3 +66,20 @@ def test_batch_refuses_bad_items(pt):
     with pytest.raises(pt.PhotonError) as e:
         pt.Batch([(g, g.camera, 32, 32, 1, 1)])
     assert e.value.status == abi.PT_ERR_UNSUPPORTED
+
+
+@pytest.mark.parametrize("strategy", ["ONE_LAUNCH", "PER_SCENE_MEGA"])
+def test_download_waits_for_a_render_on_the_callers_stream(pt, strategy):
+    """render(count_rays=False) on a caller's stream returns without waiting;
+    the download that follows must still see the finished images."""
+    import torch
+    from photon_tracer_b200 import abi
+    items = small_batch(pt)
+    want = pt.Batch(items, getattr(abi, "PT_BATCH_" + strategy))
+    want.render()
+    ref = [want.image(i) for i in range(len(items))]
+    b = pt.Batch(items, getattr(abi, "PT_BATCH_" + strategy))
+    s = torch.cuda.Stream()
+    b.render(stream=s.cuda_stream, count_rays=False)
+    assert all(b.image(i).tobytes() == ref[i].tobytes() for i in range(len(items)))
+    assert np.all(np.isfinite(b.scene_times()))

@@ -54,6 +54,34 @@ def test_noalloc_matches_scratch_entry_point(built):
         np.testing.assert_allclose(g, wnt, rtol=1e-3, atol=1e-5)
 
 
+@pytest.mark.parametrize("w,h", [(512, 512), (1024, 256)])
+def test_noalloc_at_its_pixel_limit(built, w, h):
+    """Frames of exactly PT_ATROUS_NOALLOC_MAX_PIXELS pixels fill the whole
+    built-in array: seeded random guides, against caller-owned scratch."""
+    import torch
+    from photon_tracer_b200 import abi
+    assert w * h == abi.PT_ATROUS_NOALLOC_MAX_PIXELS
+    lib = built.load()
+    stream = torch.cuda.current_stream().cuda_stream
+    gen = torch.Generator(device="cuda").manual_seed(w)
+    color = torch.rand((h, w, 3), device="cuda", generator=gen) * 3
+    albedo = torch.rand((h, w, 3), device="cuda", generator=gen)
+    normal = torch.randn((h, w, 3), device="cuda", generator=gen)
+    variance = torch.rand((h, w), device="cuda", generator=gen)
+    ptrs = [C.c_void_p(t.data_ptr()) for t in (color, albedo, normal, variance)]
+    scratch = torch.empty(lib.pt_denoise_atrous_scratch_floats(w, h), dtype=torch.float32, device="cuda")
+    want = torch.empty((h, w, 3), dtype=torch.float32, device="cuda")
+    got = torch.full((h, w, 3), float("nan"), dtype=torch.float32, device="cuda")
+    assert lib.pt_denoise_atrous_device(w, h, *ptrs, C.c_void_p(want.data_ptr()), C.c_void_p(scratch.data_ptr()),
+                                        C.c_void_p(stream)) == 0, lib.pt_last_error()
+    assert lib.pt_denoise_atrous_device_noalloc(w, h, *ptrs, C.c_void_p(got.data_ptr()), C.c_void_p(stream)) == 0, \
+        lib.pt_last_error()
+    torch.cuda.synchronize()
+    g, wnt = got.cpu().numpy(), want.cpu().numpy()
+    assert np.isfinite(g).all()
+    np.testing.assert_allclose(g, wnt, rtol=1e-3, atol=1e-5)
+
+
 def test_noalloc_refuses_frames_beyond_its_scratch(built):
     import torch
     from photon_tracer_b200 import abi

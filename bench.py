@@ -13,7 +13,9 @@ the frame: the path does not shard across GPUs in this workload, so the runs
 are replicas (weak scaling) and value is the sum of all ranks' rays over the
 slowest rank's time. --impl reference times the reference's own CPU renderer
 (oracle/_ref, built from the reference's sources; the C restatement if it is
-absent) on this host's cores on bounded row samples of the same frame.
+absent) on this host's cores over a fixed row set of the same frame (every
+8th scanline), fastest pass; cpu_baseline beside our line is the same
+measurement (best of 3 passes).
 """
 from __future__ import annotations
 
@@ -125,66 +127,75 @@ def bytes_per_ray(desc, cam):
                                                   "counts": [int(x) for x in totals]}
 
 
-def cpu_reference_rate(desc, cam, seconds: float, threads: int):
-    """The reference renderer (oracle/_ref) on this host's cores, rendering
-    rows of the same frame; returns (Mrays/s, sample description, kind, threads)."""
-    from oracle.oracle import Oracle, Reference, ref_available
-    if ref_available():
-        r, kind = Reference(desc), "reference"
-        run = lambda j0, n: r.render(cam, WIDTH, HEIGHT, SPP, DEPTH, seed=SEED, row0=j0, rows=n, threads=threads)[2]
+def cpu_reference_rate(runs: int = 3):
+    """The reference renderer on this host's cores over the fixed row set of
+    the frame (oracle/ref_arm.py), best of `runs` passes -- the same
+    measurement as the reference arm's. Returns the cpu_baseline object."""
+    from oracle import ref_arm
+    cpu = ref_arm.host_cpu()
+    if ref_arm.available():
+        frame = ref_arm.RoomMeshFrame()
+        frame.render_rows(cpu["threads"])  # warm-up pass
+        rate, passes = ref_arm.best_of(frame, runs, cpu["threads"])
+        sample, kind = frame.sample(), "reference"
+        frame.close()
     else:
-        o, kind, threads = Oracle(desc), "port", 1
-        run = lambda j0, n: o.render(cam, WIDTH, HEIGHT, SPP, DEPTH, seed=SEED, rng_mode=2, row0=j0, rows=n)[2]
-    calib = max(1, threads // 2)
-    t0 = time.perf_counter()
-    run(HEIGHT // 2, calib)
-    dt = time.perf_counter() - t0
-    rows = int(max(threads, min(HEIGHT, calib * seconds / max(dt, 1e-3))))
-    j0 = max(0, HEIGHT // 2 - rows // 2)
-    t0 = time.perf_counter()
-    rays = run(j0, rows)
-    dt = time.perf_counter() - t0
-    return rays / dt / 1e6, f"rows {j0}..{j0 + rows - 1} of the 1024x1024 frame at 64 spp ({rays} rays, {dt:.1f} s)", kind, threads
+        rate, passes, sample, kind = port_rate(runs)
+        cpu["threads"] = 1
+    return {"value": round(rate, 3), "unit": "Mrays/s", "cores": cpu["threads"], "kind": kind,
+            "sample": f"{sample}; best of {runs} passes", "cpu_model": cpu["model"],
+            "passes_s": [round(p[1], 3) for p in passes]}
+
+
+def port_rate(runs):
+    """Without the reference harness: the oracle's C restatement (one
+    thread) on 8 rows of the frame -- the only CPU path left; it needs the
+    product's generator for the scene description."""
+    import photon_tracer_b200 as pt
+    from photon_tracer_b200 import abi
+    from oracle.oracle import Oracle
+    g = pt.Generated(abi.PT_GEN_ROOM_MESH, seed=SEED)
+    o = Oracle(g.desc)
+    passes = []
+    for _ in range(runs):
+        t0 = time.perf_counter()
+        rays = sum(o.render(g.camera, WIDTH, HEIGHT, SPP, DEPTH, seed=SEED, rng_mode=2, row0=j, rows=1)[2]
+                   for j in range(4, HEIGHT, 128))
+        passes.append((rays, time.perf_counter() - t0))
+    rays, secs = min(passes, key=lambda p: p[1])
+    return rays / secs / 1e6, passes, "every 128th scanline of the 1024x1024 frame (oracle port)", "port"
 
 
 def run_reference_arm(args, rank, world):
+    """The reference's own CPU renderer (oracle/_ref) on this host's cores:
+    every step is one pass over the fixed row set of the frame; value is the
+    fastest step's Mrays/s (the statistic cpu_baseline reports). No product
+    code is loaded when the reference harness is present."""
     if rank != 0:
         return 0
-    import photon_tracer_b200 as pt
-    from photon_tracer_b200 import abi
-    from oracle.oracle import Oracle, Reference, ref_available
-    g = pt.Generated(abi.PT_GEN_ROOM_MESH, seed=SEED)
-    threads = os.cpu_count() or 1
-    if ref_available():
-        r, kind = Reference(g.desc), "reference"
-        run = lambda j0, n: r.render(g.camera, WIDTH, HEIGHT, SPP, DEPTH, seed=SEED, row0=j0, rows=n, threads=threads)[2]
+    from oracle import ref_arm
+    cpu = ref_arm.host_cpu()
+    if ref_arm.available():
+        frame = ref_arm.RoomMeshFrame()
+        for _ in range(args.warmup):
+            frame.render_rows(cpu["threads"])
+        steps = [frame.render_rows(cpu["threads"]) for _ in range(args.steps)]
+        sample, kind, threads = frame.sample(), "reference", cpu["threads"]
+        frame.close()
     else:
-        o, kind, threads = Oracle(g.desc), "port", 1
-        run = lambda j0, n: o.render(g.camera, WIDTH, HEIGHT, SPP, DEPTH, seed=SEED, rng_mode=2, row0=j0, rows=n)[2]
-    # size a step to about 4 s of CPU work
-    t0 = time.perf_counter()
-    run(HEIGHT // 2, threads)
-    dt = time.perf_counter() - t0
-    rows = int(max(threads, min(HEIGHT, threads * 4.0 / max(dt, 1e-3))))
-    steps = []
-    for k in range(args.warmup + args.steps):
-        j0 = (k * 131) % max(1, HEIGHT - rows)
-        t0 = time.perf_counter()
-        rays = run(j0, rows)
-        dt = time.perf_counter() - t0
-        if k >= args.warmup:
-            steps.append((rays, dt))
-    rays = sum(s[0] for s in steps)
-    secs = sum(s[1] for s in steps)
+        _, steps, sample, kind = port_rate(args.steps)
+        threads = 1
+    rays, secs = min(steps, key=lambda p: p[1])
     value = rays / secs / 1e6
-    sample = f"{rows} rows of the 1024x1024 frame at 64 spp per step"
+    mean = sum(p[0] for p in steps) / sum(p[1] for p in steps) / 1e6
     line = {"impl": "reference", "metric": METRIC, "value": round(value, 3), "unit": "Mrays/s", "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(secs / len(steps) * 1e3, 3),
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(secs * 1e3, 3),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": WORKLOAD, "scene": "room_mesh", "width": WIDTH, "height": HEIGHT, "spp": SPP,
-                       "depth": DEPTH, "seed": SEED, "rows_per_step": rows},
+                       "depth": DEPTH, "seed": SEED, "sample": sample},
             "cpu_baseline": {"value": round(value, 3), "unit": "Mrays/s", "cores": threads, "kind": kind,
-                             "sample": sample},
+                             "sample": f"{sample}; fastest of {args.steps} steps", "cpu_model": cpu["model"]},
+            "mean_Mrays_s": round(mean, 3),
             "e2e": {"value": round(value, 3), "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
@@ -575,8 +586,7 @@ def main():
                 traffic = None
         cpu = None
         if world == 1 and not args.no_cpu_baseline:
-            rate, sample, kind, threads = cpu_reference_rate(g.desc, g.camera, 10.0, os.cpu_count() or 1)
-            cpu = {"value": round(rate, 3), "unit": "Mrays/s", "cores": threads, "kind": kind, "sample": sample}
+            cpu = cpu_reference_rate(3)
         line = {
             "metric": METRIC, "value": round(value, 2), "unit": "Mrays/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(ms_per_launch, 3), "higher_is_better": True,

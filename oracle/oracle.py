@@ -89,6 +89,13 @@ def ref_lib() -> C.CDLL:
         L.ref_builtin_scene.argtypes = [C.c_int, C.POINTER(C.c_uint32), P, P]
         L.ref_write_image.restype = C.c_int
         L.ref_write_image.argtypes = [C.c_char_p, C.c_int, C.c_int, P]
+        L.ref_world_create.restype = P
+        L.ref_world_create.argtypes = [C.c_int, C.c_char_p, C.c_int, C.c_int, C.c_double]
+        L.ref_world_desc.restype = C.POINTER(abi.pt_scene_desc)
+        L.ref_world_desc.argtypes = [P]
+        L.ref_world_camera.restype = C.POINTER(abi.pt_camera)
+        L.ref_world_camera.argtypes = [P]
+        L.ref_world_destroy.argtypes = [P]
         _rlib = L
     return _rlib
 
@@ -226,16 +233,37 @@ class Oracle:
         except Exception:
             pass
 
-    def trace_closest(self, rays, tmin=0.001, tmax=1000.0, counts=False):
+    @staticmethod
+    def _chunks(n, threads):
+        """Contiguous [a, b) ranges for `threads` workers (ctypes calls release
+        the GIL, and the oracle's ray queries only read the scene)."""
+        step = max(1, -(-n // max(1, threads)))
+        return [(a, min(n, a + step)) for a in range(0, n, step)]
+
+    def trace_closest(self, rays, tmin=0.001, tmax=1000.0, counts=False, threads=1):
         rays = np.ascontiguousarray(rays, np.float32).reshape(-1, 6)
         out = np.empty(len(rays), abi.HIT_DTYPE)
         c = np.zeros(5, np.uint64)
+        if threads > 1 and not counts and len(rays) > threads:
+            from concurrent.futures import ThreadPoolExecutor
+            with ThreadPoolExecutor(threads) as ex:
+                list(ex.map(lambda ab: self.lib.po_trace_closest(self.h, _ptr(rays[ab[0]:ab[1]]), ab[1] - ab[0], tmin,
+                                                                 tmax, _ptr(out[ab[0]:ab[1]]), None),
+                            self._chunks(len(rays), threads)))
+            return out
         self.lib.po_trace_closest(self.h, _ptr(rays), len(rays), tmin, tmax, _ptr(out), _ptr(c) if counts else None)
         return (out, c) if counts else out
 
-    def trace_any(self, rays, tmin=0.001, tmax=1000.0):
+    def trace_any(self, rays, tmin=0.001, tmax=1000.0, threads=1):
         rays = np.ascontiguousarray(rays, np.float32).reshape(-1, 6)
         out = np.empty(len(rays), np.uint8)
+        if threads > 1 and len(rays) > threads:
+            from concurrent.futures import ThreadPoolExecutor
+            with ThreadPoolExecutor(threads) as ex:
+                list(ex.map(lambda ab: self.lib.po_trace_any(self.h, _ptr(rays[ab[0]:ab[1]]), ab[1] - ab[0], tmin, tmax,
+                                                             _ptr(out[ab[0]:ab[1]])),
+                            self._chunks(len(rays), threads)))
+            return out
         self.lib.po_trace_any(self.h, _ptr(rays), len(rays), tmin, tmax, _ptr(out))
         return out
 
@@ -343,3 +371,31 @@ def ref_camera(lookfrom, lookat, vfov):
     cam = abi.pt_camera()
     ref_lib().ref_camera(abi.f3(lookfrom), abi.f3(lookat), vfov, C.byref(cam))
     return cam
+
+
+class RefWorld:
+    """One of the reference's own worlds as its CLI builds it (build_world in
+    include/renderer.hpp:335-343, src/main.cpp:63-108): scene id 0 materials,
+    1 field, 2 mesh (the OBJ between two spheres), 3 room, 4 crowd (side x
+    side copies of the OBJ, flattened or instanced), with NEE on. desc points
+    into the reference's geometry (trees included); camera is make_camera(id)."""
+
+    MATERIALS, FIELD, MESH, ROOM, CROWD = 0, 1, 2, 3, 4
+
+    def __init__(self, scene_id: int, obj_path: str = "", crowd_side: int = 20, flatten: bool = False,
+                 turn_deg: float = 0.0):
+        self.lib = ref_lib()
+        self.h = self.lib.ref_world_create(scene_id, obj_path.encode(), crowd_side, int(flatten), turn_deg)
+        self.desc = self.lib.ref_world_desc(self.h).contents
+        self.camera = abi.pt_camera.from_buffer_copy(self.lib.ref_world_camera(self.h).contents)
+
+    def close(self):
+        if self.h:
+            self.lib.ref_world_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -11,14 +11,19 @@
 // value private (geometry::hit's choice of primitive, the camera's aspect),
 // the harness re-composes it from public pieces and cross-checks the result
 // against the reference's own call.
+#include <array>
 #include <atomic>
 #include <cstring>
+#include <map>
+#include <fstream>
+#include <sstream>
 #include <thread>
 #include <vector>
 
 #include "image_write.hpp"
 #include "renderer.hpp"
 #include "../include/photon_cuda.h"
+#include "../include/photon_cuda_geometry.hpp"
 
 namespace {
 
@@ -357,3 +362,216 @@ extern "C" {
 // The reference's write_image (include/image_write.hpp:15-33).
 int ref_write_image(const char* path, int w, int h, const float* linear) { return write_image(path, w, h, linear) ? 1 : 0; }
 }
+
+extern "C" {
+// The reference's own worlds as its CLI builds them (src/main.cpp:63-108):
+// build_world(id, use_bvh, the OBJ's text, a reader for the files beside it,
+// turn, crowd side, flatten) with NEE on, exported in the C ABI's layout by
+// photon_cuda_geometry.hpp (the trees geometry::build made included), with
+// make_camera(id). For writing fixtures of the reference's OBJ scenes (the
+// teapot, the crowd and its flattened form, the spot crowd).
+struct ref_world {
+    geometry world;
+    photon_cuda::scene_arrays arrays;
+    pt_camera cam;
+};
+
+static std::string read_file(const std::string& path) {
+    std::ifstream f(path, std::ios::binary);
+    if (!f) return std::string();
+    std::ostringstream buf;
+    buf << f.rdbuf();
+    return buf.str();
+}
+
+void* ref_world_create(int id, const char* obj_path, int crowd_side, int flatten, double turn_deg) {
+    const std::string path = obj_path ? obj_path : "";
+    const std::string dir = path.find('/') == std::string::npos ? "" : path.substr(0, path.find_last_of('/') + 1);
+    const std::string text = path.empty() ? std::string() : read_file(path);
+    const file_reader beside = [dir](const std::string& name) { return read_file(dir + name); };
+    auto* w = new ref_world();
+    const scene_id sid = static_cast<scene_id>(id);
+    w->world = build_world(sid, sid != scene_id::materials, text, beside, turn_deg, crowd_side, flatten != 0);
+    w->world.sample_lights = true;
+    w->arrays.from(w->world);
+    w->cam = photon_cuda::camera_of(make_camera(sid));
+    return w;
+}
+
+const pt_scene_desc* ref_world_desc(void* h) { return &static_cast<ref_world*>(h)->arrays.desc; }
+const pt_camera* ref_world_camera(void* h) { return &static_cast<ref_world*>(h)->cam; }
+void ref_world_destroy(void* h) { delete static_cast<ref_world*>(h); }
+}  // extern "C"
+
+// ---- the room-mesh benchmark frame, built through the reference's own API ----------------
+// A restatement, in the reference's classes and float arithmetic, of this
+// project's room-mesh generator (the closed room without a front wall, a
+// ceiling lamp, a glass sphere and a radially displaced icosphere with
+// area-weighted vertex normals, include/obj.hpp:198-204), so the reference
+// arm of the benchmark renders the frame without loading any product code.
+// tests/test_ref_arm.py checks it equal, byte for byte, to the product's
+// generated description.
+namespace {
+uint32_t rm_hash32(uint32_t x) {
+    x ^= x >> 16; x *= 0x7feb352du;
+    x ^= x >> 15; x *= 0x846ca68bu;
+    x ^= x >> 16;
+    return x;
+}
+double rm_lattice(int i, int j, int k, uint32_t seed) {
+    uint32_t h = rm_hash32(seed ^ 0x9e3779b9u);
+    h = rm_hash32(h ^ uint32_t(i) * 0x8da6b343u);
+    h = rm_hash32(h ^ uint32_t(j) * 0xd8163841u);
+    h = rm_hash32(h ^ uint32_t(k) * 0xcb1ab31fu);
+    return (h >> 8) * (2.0 / 16777216.0) - 1.0;
+}
+double rm_noise(double x, double y, double z, uint32_t seed) {
+    const double fx = std::floor(x), fy = std::floor(y), fz = std::floor(z);
+    const int ix = int(fx), iy = int(fy), iz = int(fz);
+    auto s = [](double t) { return t * t * (3 - 2 * t); };
+    const double tx = s(x - fx), ty = s(y - fy), tz = s(z - fz);
+    double acc = 0;
+    for (int c = 0; c < 8; ++c) {
+        const int dx = c & 1, dy = (c >> 1) & 1, dz = (c >> 2) & 1;
+        acc += (dx ? tx : 1 - tx) * (dy ? ty : 1 - ty) * (dz ? tz : 1 - tz) * rm_lattice(ix + dx, iy + dy, iz + dz, seed);
+    }
+    return acc;
+}
+double rm_fbm4(double x, double y, double z, uint32_t seed) {
+    double sum = 0, amp = 1, f = 2.0;
+    for (int o = 0; o < 4; ++o) {
+        sum += amp * rm_noise(x * f, y * f, z * f, seed + 101u * uint32_t(o));
+        amp *= 0.5;
+        f *= 2;
+    }
+    return sum;
+}
+point3 rm_p(double x, double y, double z) { return point3(float(x), float(y), float(z)); }
+
+void room_mesh_world(geometry& w, uint64_t seed, int subdiv) {
+    w.sky = false;
+    const material* white = w.own(std::make_shared<lambertian>(color(0.73f, 0.73f, 0.73f)));
+    const material* red = w.own(std::make_shared<lambertian>(color(0.65f, 0.05f, 0.05f)));
+    const material* green = w.own(std::make_shared<lambertian>(color(0.12f, 0.45f, 0.15f)));
+    add_quad(w, rm_p(-1, -1, 1), rm_p(2, 0, 0), rm_p(0, 0, -2), white);
+    add_quad(w, rm_p(-1, 1, 1), rm_p(2, 0, 0), rm_p(0, 0, -2), white);
+    add_quad(w, rm_p(-1, -1, -1), rm_p(2, 0, 0), rm_p(0, 2, 0), white);
+    add_quad(w, rm_p(-1, -1, 1), rm_p(0, 0, -2), rm_p(0, 2, 0), red);
+    add_quad(w, rm_p(1, -1, 1), rm_p(0, 0, -2), rm_p(0, 2, 0), green);
+    w.spheres.emplace_back(rm_p(0, 0.82, -0.1), 0.15f, w.own(std::make_shared<diffuse_light>(color(15, 15, 15))));
+    w.spheres.emplace_back(rm_p(0.5, -0.8, 0.35), 0.2f, w.own(std::make_shared<dielectric>(1.5f)));
+    // icosphere: 12 corners, then midpoints pushed out to the unit sphere, in double
+    std::vector<std::array<double, 3>> v;
+    const double t = (1.0 + std::sqrt(5.0)) / 2.0;
+    const double base[12][3] = {{-1, t, 0}, {1, t, 0}, {-1, -t, 0}, {1, -t, 0}, {0, -1, t}, {0, 1, t},
+                                {0, -1, -t}, {0, 1, -t}, {t, 0, -1}, {t, 0, 1}, {-t, 0, -1}, {-t, 0, 1}};
+    for (auto& p : base) {
+        const double l = std::sqrt(p[0] * p[0] + p[1] * p[1] + p[2] * p[2]);
+        v.push_back({p[0] / l, p[1] / l, p[2] / l});
+    }
+    std::vector<std::array<uint32_t, 3>> f = {{0, 11, 5}, {0, 5, 1}, {0, 1, 7}, {0, 7, 10}, {0, 10, 11},
+                                              {1, 5, 9}, {5, 11, 4}, {11, 10, 2}, {10, 7, 6}, {7, 1, 8},
+                                              {3, 9, 4}, {3, 4, 2}, {3, 2, 6}, {3, 6, 8}, {3, 8, 9},
+                                              {4, 9, 5}, {2, 4, 11}, {6, 2, 10}, {8, 6, 7}, {9, 8, 1}};
+    for (int s = 0; s < subdiv; ++s) {
+        std::map<std::pair<uint32_t, uint32_t>, uint32_t> mid;
+        auto midpoint = [&](uint32_t a, uint32_t b) {
+            const auto key = std::make_pair(std::min(a, b), std::max(a, b));
+            auto it = mid.find(key);
+            if (it != mid.end()) return it->second;
+            double p[3];
+            for (int k = 0; k < 3; ++k) p[k] = 0.5 * (v[a][k] + v[b][k]);
+            const double l = std::sqrt(p[0] * p[0] + p[1] * p[1] + p[2] * p[2]);
+            v.push_back({p[0] / l, p[1] / l, p[2] / l});
+            mid.emplace(key, uint32_t(v.size() - 1));
+            return uint32_t(v.size() - 1);
+        };
+        std::vector<std::array<uint32_t, 3>> next;
+        for (const auto& q : f) {
+            const uint32_t a = midpoint(q[0], q[1]), b = midpoint(q[1], q[2]), c = midpoint(q[2], q[0]);
+            next.push_back({q[0], a, c});
+            next.push_back({q[1], b, a});
+            next.push_back({q[2], c, b});
+            next.push_back({a, b, c});
+        }
+        f.swap(next);
+    }
+    // radial displacement: radius 0.45 * (1 + (0.05 / 0.45) * fbm4(direction)) about (-0.2, -0.5, -0.25)
+    const double center[3] = {-0.2, -0.5, -0.25}, radius = 0.45, amp = 0.05 / 0.45;
+    std::vector<point3> pos;
+    for (auto& p : v) {
+        const double r = radius * (1.0 + amp * rm_fbm4(p[0], p[1], p[2], static_cast<uint32_t>(seed)));
+        pos.push_back(rm_p(center[0] + r * p[0], center[1] + r * p[1], center[2] + r * p[2]));
+    }
+    std::vector<vec3> acc(pos.size(), vec3(0, 0, 0));
+    for (const auto& q : f) {
+        const vec3 n = cross(pos[q[1]] - pos[q[0]], pos[q[2]] - pos[q[0]]);
+        for (int k = 0; k < 3; ++k) acc[q[k]] = acc[q[k]] + n;
+    }
+    const material* clay = w.own(std::make_shared<lambertian>(color(0.8f, 0.8f, 0.8f)));
+    for (const auto& q : f)
+        w.triangles.emplace_back(pos[q[0]], pos[q[1]], pos[q[2]], acc[q[0]].normalize(), acc[q[1]].normalize(),
+                                 acc[q[2]].normalize(), clay);
+}
+
+// camera.hpp:18-34 with the aspect ratio a parameter (1 for the square frame).
+camera square_camera(point3 from, point3 at, double vfov_deg, double aspect) {
+    const double viewport_height = 2.0 * std::tan(vfov_deg * M_PI / 360.0);
+    const double viewport_width = aspect * viewport_height;
+    const vec3 w = (from - at).normalize();
+    const vec3 u = cross(vec3(0, 1, 0), w).normalize();
+    const vec3 v = cross(w, u);
+    pt_camera c;
+    const vec3 horizontal = u * viewport_width, vertical = v * viewport_height;
+    const point3 llc = from - (horizontal * 0.5) - (vertical * 0.5) - w;
+    for (int a = 0; a < 3; ++a) {
+        c.origin[a] = from.e[a];
+        c.lower_left[a] = llc.e[a];
+        c.horizontal[a] = horizontal.e[a];
+        c.vertical[a] = vertical.e[a];
+    }
+    return camera_from(&c);
+}
+}  // namespace
+
+extern "C" {
+// The room-mesh frame's scene (icosphere subdivision `subdiv`, noise seed
+// `seed`) and its camera (from (0, 0, 3.3) at the origin, vfov 40, square),
+// built by the reference's geometry::build with its BVH.
+void* ref_room_mesh_world(uint64_t seed, int subdiv) {
+    auto* w = new ref_world();
+    room_mesh_world(w->world, seed, subdiv);
+    w->world.sample_lights = true;
+    w->world.build(true);
+    w->arrays.from(w->world);
+    w->cam = photon_cuda::camera_of(square_camera(rm_p(0, 0, 3.3), rm_p(0, 0, 0), 40.0, 1.0));
+    return w;
+}
+
+// render_row_linear over the listed scanlines (j counted from the bottom)
+// on `threads` threads taking rows from an atomic counter (src/main.cpp:137-158);
+// out gets each row at its place in a W x H frame (top row first) or is
+// NULL. Returns the ray count.
+uint64_t ref_world_render_rows(void* h, int W, int H, int spp, int depth, uint64_t seed, const int* rows,
+                               int n_rows, float* out, int threads) {
+    const ref_world* rw = static_cast<ref_world*>(h);
+    const camera cam = camera_from(&rw->cam);
+    std::atomic<int> next{0};
+    std::atomic<long long> total{0};
+    auto worker = [&]() {
+        rays_traced = 0;
+        std::vector<float> row(3 * size_t(W));
+        for (int k = next.fetch_add(1); k < n_rows; k = next.fetch_add(1)) {
+            const int j = rows[k];
+            float* dst = out ? out + 3 * size_t(H - 1 - j) * W : row.data();
+            render_row_linear(rw->world, cam, j, W, H, spp, depth, dst, seed, 0, nullptr);
+        }
+        total += rays_traced;
+    };
+    std::vector<std::thread> pool;
+    for (int t = 1; t < threads; ++t) pool.emplace_back(worker);
+    worker();
+    for (auto& t : pool) t.join();
+    return uint64_t(total.load());
+}
+}  // extern "C"

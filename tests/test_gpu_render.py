@@ -65,6 +65,27 @@ def test_snapshot_render_matches_reference(pt, name):
     assert abs(int(rays) - int(f["rays"])) <= 0.01 * int(f["rays"])
 
 
+@pytest.mark.parametrize("seed", range(4))
+def test_snapshot_material_renders_match_reference(pt, seed):
+    """The reference's renders of random-material scenes -- metal fuzz above 1
+    (clamped to 1 by its constructor), dielectric ior at and below 1, negative
+    radii, emitters -- replayed on the GPU from the reference's own per-row
+    stream: image, guides and ray count at the render bars."""
+    from handmade import random_material_scene
+    from photon_tracer_b200 import abi
+    f = golden("ref_material_renders.npz")
+    d, cam = random_material_scene(pt, 500 + seed)
+    s = pt.Scene(d.desc_ptr)
+    img, aux, rays = s.render(cam, 24, 16, 4, 10, seed=seed, rng=abi.PT_RNG_SNAPSHOT, states=f[f"s{seed}_states"],
+                              aux=True, mode=abi.PT_MODE_MEGAKERNEL)
+    assert_render_close(img, f[f"s{seed}_image"], f"materials {seed}")
+    assert_render_close(aux, f[f"s{seed}_aux"], f"materials {seed} aux")
+    assert abs(int(rays) - int(f[f"s{seed}_rays"])) <= 0.01 * int(f[f"s{seed}_rays"])
+    wf = s.render(cam, 24, 16, 4, 10, seed=seed, rng=abi.PT_RNG_SNAPSHOT, states=f[f"s{seed}_states"], aux=True,
+                  mode=abi.PT_MODE_WAVEFRONT)
+    assert wf[0].tobytes() == img.tobytes() and wf[1].tobytes() == aux.tobytes() and wf[2] == rays
+
+
 @pytest.mark.parametrize("kind,param,w,h,spp", [
     ("ROOM_MESH", 6, 64, 64, 4), ("RANDOM_SPHERES", 0, 80, 45, 4), ("INSTANCES", 0, 64, 36, 2),
     ("REF_ROOM", 0, 64, 36, 4), ("REF_MATERIALS", 0, 64, 36, 4), ("TEXTURED", 0, 64, 36, 4),
@@ -175,20 +196,31 @@ def block_z(image, mean, sigma, seeds, block=20, floor=2e-4):
             float(np.max(np.abs(d3.sum(axis=(0, 1)) / np.sqrt(v3.sum(axis=(0, 1)))))))
 
 
-@pytest.mark.parametrize("scene,gen", [("materials", "REF_MATERIALS"), ("field", "REF_FIELD"), ("room", "REF_ROOM")])
+@pytest.mark.parametrize("scene,gen", [("materials", "REF_MATERIALS"), ("field", "REF_FIELD"), ("room", "REF_ROOM"),
+                                       ("teapot", "teapot"), ("crowd", "crowd"), ("crowd", "crowd, flattened"),
+                                       ("spot_crowd", "spot_crowd")])
 def test_reference_statistical_fixture(pt, scene, gen):
     """The reference's own render regression (tests/render_test.py check with
     tests/reference.json): 960x540, 200 spp, seed 1, |z| <= 10 per block,
-    6 per block row, 5 per image."""
+    6 per block row, 5 per image. The OBJ scenes (the teapot; the crowd of 64
+    instanced teapots; the same crowd flattened into world-space triangles,
+    which must match the instanced crowd's reference -- the reference's check
+    of instance transforms, normals and inverses; the textured spot crowd)
+    come from fixtures of the reference's own scene descriptions."""
     from photon_tracer_b200 import abi
+    from scene_fixture import FixtureScene
     f = golden("reference_blocks.npz")
     meta = json.loads(str(f["meta"]))
-    g = pt.Generated(getattr(abi, "PT_GEN_" + gen))
-    s = pt.Scene(g)
+    if gen.startswith(("teapot", "crowd", "spot")):
+        g = FixtureScene(golden(f"ref_scene_{scene}.npz"), flatten=gen.endswith("flattened"))
+        s = pt.Scene(g.desc_ptr)
+    else:
+        g = pt.Generated(getattr(abi, "PT_GEN_" + gen))
+        s = pt.Scene(g)
     w = meta["width"]
     img, _, _ = s.render(g.camera, w, int(w / (16 / 9)), meta["spp"], 10, seed=1)
     b, r, i = block_z(img, f[f"{scene}_mean"], f[f"{scene}_sigma"], meta["seeds"])
-    assert b <= 10 and r <= 6 and i <= 5, (scene, b, r, i)
+    assert b <= 10 and r <= 6 and i <= 5, (gen, b, r, i)
 
 
 def test_denoise_matches_oracle(pt):

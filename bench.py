@@ -111,20 +111,111 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def bytes_per_ray(desc, cam):
+def bytes_per_ray(desc, cam, width=WIDTH, height=HEIGHT, spp=SPP):
     """Algorithmic bytes per counted ray from the CPU oracle's traversal
-    counters on a bounded sample of the frame (8 rows at full spp)."""
+    counters on a bounded sample of the frame (8 rows at `spp`)."""
     from oracle.oracle import Oracle
     o = Oracle(desc)
-    rows = [int(HEIGHT * (k + 0.5) / 8) for k in range(8)]
+    rows = [int(height * (k + 0.5) / 8) for k in range(8)]
     totals = np.zeros(5, np.float64)
     rays = 0
     for j in rows:
-        _, _, r, c = o.render(cam, WIDTH, HEIGHT, SPP, DEPTH, seed=SEED, rng_mode=0, row0=j, rows=1, counts=True)
+        _, _, r, c = o.render(cam, width, height, spp, DEPTH, seed=SEED, rng_mode=0, row0=j, rows=1, counts=True)
         totals += c
         rays += r
     return float((totals * BYTES).sum() / rays), {"rays": int(rays), "rows": rows,
                                                   "counts": [int(x) for x in totals]}
+
+
+def l2_copy_peak(stream):
+    """A measured L2 bandwidth reference: a device copy between two 24 MB
+    buffers that stay resident in the 126 MB L2, timed with CUDA events on
+    `stream` over 200 copies after warm-up; GB/s of bytes read + written."""
+    import torch
+    n = 6 << 20  # floats: 24 MB per buffer
+    with torch.cuda.stream(stream):
+        a = torch.rand(n, device="cuda")
+        b = torch.empty_like(a)
+        for _ in range(20):
+            b.copy_(a)
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record(stream)
+        for _ in range(200):
+            b.copy_(a)
+        e.record(stream)
+        stream.synchronize()
+    return 2 * 4 * n * 200 / (s.elapsed_time(e) / 1e3) / 1e9
+
+
+def instanced_frame(args, stream, flush, peak):
+    """The 10,000-instance frame (1920x1080, 32 spp, depth 10, NEE) through
+    pt_render_device: Mrays/s over K frames (L2 flushed between them, CUDA
+    events on the launching stream) and its bytes-per-ray roofline (oracle
+    counters on 8 rows at 4 spp)."""
+    import torch
+    import photon_tracer_b200 as pt
+    from photon_tracer_b200 import abi
+    g = pt.Generated(abi.PT_GEN_INSTANCES, seed=SEED)
+    scene = pt.Scene(g)
+    st = pt.Scene.settings(g.width, g.height, g.spp, DEPTH, SEED, 0, abi.PT_MODE_MEGAKERNEL, abi.PT_RNG_SAMPLE)
+    out = torch.empty((g.height, g.width, 3), dtype=torch.float32, device="cuda")
+    rays = torch.zeros(1, dtype=torch.int64, device="cuda")
+    steps = max(3, min(args.steps, 10))
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            flush.zero_()
+            scene.render_device(g.camera, st, out.data_ptr(), 0, rays.data_ptr(), stream.cuda_stream)
+        scene.sync(stream.cuda_stream)
+        rays.zero_()
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+        for a, b in ev:
+            flush.zero_()
+            a.record(stream)
+            scene.render_device(g.camera, st, out.data_ptr(), 0, rays.data_ptr(), stream.cuda_stream)
+            b.record(stream)
+        stream.synchronize()
+        scene.sync(stream.cuda_stream)
+    ms = sum(a.elapsed_time(b) for a, b in ev)
+    n_rays = int(rays.item())
+    bpr, info = bytes_per_ray(g.desc, g.camera, g.width, g.height, 4)
+    achieved = bpr * (n_rays / steps) / (ms / steps / 1e3) / 1e9
+    scene.close()
+    return {"workload": "10,000 instances of three meshes (201,552 tris), 1920x1080, 32 spp, depth 10, NEE",
+            "value": round(n_rays / ms / 1e3, 2), "unit": "Mrays/s", "ms_per_step": round(ms / steps, 3),
+            "steps": steps, "kernel": "megakernel (single loop over all trees)",
+            "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                         "frac": round(achieved / peak, 4), "bytes_per_ray": round(bpr, 2),
+                         "note": "bytes per ray counted by the CPU oracle on 8 rows at 4 spp"}}
+
+
+def convergence_summary():
+    """Time to relMSE <= 0.01 at 1920x1080 on one held-out seed (1001) per
+    scene generator, against FP64 ground truth of 1,024 spp (its own relMSE
+    is ~0.2-0.7 / 1024, under 7% of the threshold): plain path tracing, the
+    a-trous filter and the learned U-Net, GPU event times."""
+    from photon_tracer_b200 import denoiser, metrics
+    w, h = 1920, 1080
+    net = denoiser.trained() if os.path.exists(denoiser.WEIGHTS) else None
+    out = {}
+    for kind in ("spheres", "room", "instances"):
+        g, scene, cam = denoiser.scene_and_camera(kind, 1001, w / h, jitter=False)
+        gt = metrics.GroundTruth(scene, cam, w, h, seed=1001, pass_spp=256)
+        gt.add(4)
+        truth = gt.image()
+        r = {"gt_spp": gt.spp}
+        for leg, kw in (("plain", dict(denoise=None, max_spp=512)), ("atrous", dict(denoise="atrous", max_spp=256)),
+                        ("unet", dict(denoise="unet", max_spp=256, net=net))):
+            if leg == "unet" and net is None:
+                continue
+            t = metrics.time_to_error(scene, cam, w, h, truth, seed=1001, **kw)
+            r[leg] = {"spp": t["spp"], "ms": None if t["ms"] is None else round(t["ms"], 2),
+                      "relmse": round(t["relmse"], 5)}
+        for leg in ("atrous", "unet"):
+            if leg in r and r[leg]["ms"] and r["plain"]["ms"]:
+                r[f"speedup_{leg}"] = round(r["plain"]["ms"] / r[leg]["ms"], 2)
+        out[kind] = r
+        scene.close()
+    return out
 
 
 def cpu_reference_rate(runs: int = 3):
@@ -202,16 +293,18 @@ def run_reference_arm(args, rank, world):
 
 
 def run_profile_case(args):
-    """The case ncu captures are taken on: the same scene and resolution at
-    4 spp (1/16 of a step's work, so every lane still renders many pixels),
-    rendered three times with the chosen kernel."""
+    """The case ncu captures are taken on: the workload's scene and resolution
+    at 4 spp (1/16 of the room step's work, 1/8 of the instanced frame's, so
+    every lane still renders many pixels), rendered three times with the
+    chosen kernel."""
     import torch
     import photon_tracer_b200 as pt
     from photon_tracer_b200 import abi
-    g = pt.Generated(abi.PT_GEN_ROOM_MESH, seed=SEED)
+    kind = abi.PT_GEN_INSTANCES if args.workload == "instances" else abi.PT_GEN_ROOM_MESH
+    g = pt.Generated(kind, seed=SEED)
     scene = pt.Scene(g)
     mode = abi.PT_MODE_MEGAKERNEL if args.mode == "mega" else abi.PT_MODE_WAVEFRONT
-    w, h, spp = WIDTH, HEIGHT, 4
+    w, h, spp = g.width, g.height, 4
     st = pt.Scene.settings(w, h, spp, DEPTH, SEED, 0, mode, abi.PT_RNG_SAMPLE)
     out = torch.empty((h, w, 3), dtype=torch.float32, device="cuda")
     rays = torch.zeros(1, dtype=torch.int64, device="cuda")
@@ -219,7 +312,8 @@ def run_profile_case(args):
     for _ in range(3):
         scene.render_device(g.camera, st, out.data_ptr(), 0, rays.data_ptr(), stream)
     scene.sync(stream)
-    print(json.dumps({"profile_case": f"{w}x{h} at {spp} spp x3", "mode": args.mode, "rays": int(rays.item())}))
+    print(json.dumps({"profile_case": f"{args.workload} {w}x{h} at {spp} spp x3", "mode": args.mode,
+                      "rays": int(rays.item())}))
     return 0
 
 
@@ -465,6 +559,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--mode", default="mega", choices=["mega", "wave"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the instanced-frame and time-to-relMSE sub-records of the default line")
     ap.add_argument("--workload", default="room",
                     choices=["room", "batch", "convergence", "unet", "bvh", "instances", "spheres"],
                     help="room: the headline line (room + displaced icosphere, 1024x1024, 64 spp); "
@@ -587,6 +683,9 @@ def main():
         cpu = None
         if world == 1 and not args.no_cpu_baseline:
             cpu = cpu_reference_rate(3)
+        l2_peak = l2_copy_peak(stream)
+        inst = instanced_frame(args, stream, flush, peak) if world == 1 and not args.no_extras else None
+        conv = convergence_summary() if world == 1 and not args.no_extras else None
         line = {
             "metric": METRIC, "value": round(value, 2), "unit": "Mrays/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(ms_per_launch, 3), "higher_is_better": True,
@@ -605,9 +704,13 @@ def main():
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 4), "traffic": traffic, "peak_kind": peak_kind,
                          "bytes_per_ray": round(bpr, 2), "kernel": "megakernel",
+                         "l2": {"peak": round(l2_peak, 1), "frac": round(achieved / l2_peak, 4),
+                                "how": "measured here: device copy between two 24 MB buffers resident in L2"},
                          "note": "algorithmic bytes = 128*nodes + 4*order + 36*tris + 16*spheres + 52*instances "
                                  "per ray, counted by the CPU oracle's traversal on 8 rows of the frame; the "
                                  "scene (~7 MB) is L2-resident, so frac is against HBM but served from L2"},
+            "instances": inst,
+            "convergence": conv,
             "cpu_baseline": cpu,
             "gpu_launches": args.steps,
             "clocks": clocks.summary(),

@@ -215,6 +215,30 @@ enum { PT_MODE_AUTO = 0, PT_MODE_MEGAKERNEL = 1, PT_MODE_WAVEFRONT = 2 };
  * per-row stream (src/main.cpp:150 -> include/renderer.hpp:349-351). */
 enum { PT_RNG_SAMPLE = 0, PT_RNG_SNAPSHOT = 1 };
 
+/* Flags of pt_settings. 0 renders exactly the reference's estimator.
+ *
+ * PT_FLAG_NEE_EXTENDED -- beyond the reference, which names both as known
+ * limits (README.md:453-456): next-event estimation toward emissive
+ * triangles, and from rough metal. With it:
+ *   - the light list is every emissive light sphere (as the reference's) plus
+ *     every emissive triangle of the flat triangle list (not those inside
+ *     meshes placed by instances); a light is picked with probability
+ *     proportional to its power (luminance of the emission times its area)
+ *     instead of uniformly among spheres;
+ *   - a light sphere is sampled over its cone as include/renderer.hpp:41-80
+ *     does, a triangle uniformly over its area; matte surfaces use these
+ *     samples as the reference does (light hit afterwards not counted again);
+ *   - metal with fuzz above 1e-3 also samples a light and weights that sample
+ *     and its own scattered ray by the power heuristic (multiple importance
+ *     sampling), with the exact density of its fuzz-ball lobe;
+ *   - glass and fuzz-0 metal reflect or refract into one direction only, so
+ *     no light sample can reach them: their light still arrives through
+ *     their scattered rays, as in the reference.
+ * It renders with the megakernel and production streams: with
+ * PT_MODE_WAVEFRONT or PT_RNG_SNAPSHOT the call fails with PT_ERR_UNSUPPORTED.
+ * Batches and the row call (pt_render_row) render without it. */
+enum { PT_FLAG_NEE_EXTENDED = 1 };
+
 typedef struct pt_settings {
     int32_t width, height;
     int32_t spp;          /* samples_per_pixel */
@@ -223,7 +247,7 @@ typedef struct pt_settings {
     int32_t first_sample; /* progressive continuation, include/renderer.hpp:411-413 */
     int32_t mode;         /* PT_MODE_* */
     int32_t rng;          /* PT_RNG_* */
-    int32_t reserved;
+    int32_t flags;        /* PT_FLAG_*; 0: the reference's estimator */
     const uint64_t* rng_states; /* PT_RNG_SNAPSHOT only: width*height*spp*4 words */
 } pt_settings;
 
@@ -473,7 +497,8 @@ enum {
     PT_GEN_ROOM_MESH = 11,      /* closed room + displaced icosphere (subdivisions = param) */
     PT_GEN_INSTANCES = 12,      /* 10,000 instances of three procedural meshes */
     PT_GEN_BATCH_SCENE = 13,    /* one scene of the 64-scene batch, by seed */
-    PT_GEN_TEXTURED = 14        /* the room with textured walls, sphere and instanced meshes, seed */
+    PT_GEN_TEXTURED = 14,       /* the room with textured walls, sphere and instanced meshes, seed */
+    PT_GEN_MESH_LIGHT = 15      /* the room lit by emissive triangle meshes, rough metal (extended NEE) */
 };
 typedef struct pt_gen_params {
     int32_t kind;

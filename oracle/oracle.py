@@ -53,6 +53,9 @@ def oracle_lib() -> C.CDLL:
         L.po_sample_stream_seed.restype = C.c_uint64
         L.po_sample_stream_seed.argtypes = [C.c_uint64, C.c_int, C.c_int, C.c_uint32]
         L.po_denoise.argtypes = [C.c_int, C.c_int, P, P, P, P, P]
+        L.po_render_flags.argtypes = L.po_render.argtypes + [C.c_int]
+        L.po_metal_lobe_pdf.restype = C.c_float
+        L.po_metal_lobe_pdf.argtypes = [abi.F3, C.c_float, abi.F3]
     return _olib
 
 
@@ -268,16 +271,18 @@ class Oracle:
         return out
 
     def render(self, cam, width, height, spp, depth=10, seed=1, first_sample=0, rng_mode=0, states=None,
-               row0=0, rows=None, aux=False, counts=False):
-        """rng_mode 0: per-sample streams, 1: snapshot states, 2: the reference's per-row stream."""
+               row0=0, rows=None, aux=False, counts=False, flags=0):
+        """rng_mode 0: per-sample streams, 1: snapshot states, 2: the reference's per-row stream.
+        flags: PT_FLAG_* (PT_FLAG_NEE_EXTENDED: the extended light sampling)."""
         rows = height - row0 if rows is None else rows
         out = np.zeros((height, width, 3), np.float32)
         ax = np.zeros((height, width, 7), np.float32) if aux else None
         rays = C.c_uint64()
         c = np.zeros(5, np.uint64)
         st = None if states is None else np.ascontiguousarray(states, np.uint64)
-        self.lib.po_render(self.h, C.byref(cam), width, height, spp, depth, seed, first_sample, rng_mode, _ptr(st),
-                           row0, rows, _ptr(out), _ptr(ax), C.byref(rays), _ptr(c) if counts else None)
+        self.lib.po_render_flags(self.h, C.byref(cam), width, height, spp, depth, seed, first_sample, rng_mode,
+                                 _ptr(st), row0, rows, _ptr(out), _ptr(ax), C.byref(rays), _ptr(c) if counts else None,
+                                 flags)
         res = (out, ax, rays.value)
         return res + (c,) if counts else res
 
@@ -399,3 +404,8 @@ class RefWorld:
             self.close()
         except Exception:
             pass
+
+
+def oracle_metal_lobe_pdf(mirror, fuzz, w):
+    """The oracle's density of metal's scattered direction at unit direction w."""
+    return float(oracle_lib().po_metal_lobe_pdf(abi.f3(mirror), float(fuzz), abi.f3(w)))

@@ -62,9 +62,34 @@ typedef struct po_scene {
     uint32_t* lights;
     uint32_t n_lights;
     float** texels; /* per texture: linear RGB (image_texture's texels, texture.hpp:13-21) */
+    /* The extended light list (PT_FLAG_NEE_EXTENDED, beyond the reference):
+     * emissive flat triangles of positive area, after the light spheres, and
+     * the cumulative pick probabilities of all of them. */
+    uint32_t* tri_lights;
+    float* tri_area;
+    uint32_t n_tri_lights;
+    float* light_cdf;
+    float pick_uniform, pick_power;
 } po_scene;
 
 static int emits(const pt_material* m) { return m->emission[0] > 0 || m->emission[1] > 0 || m->emission[2] > 0; }
+
+/* Power of a light for the extended pick: luminance of the emission times
+ * the area (4 pi r^2 for a sphere), 0 when not positive and finite; half the
+ * pick probability is uniform over the lights, half in proportion to power. */
+static float light_lum(const float* e) { return 0.2126f * e[0] + 0.7152f * e[1] + 0.0722f * e[2]; }
+static float sphere_power(float lum, float r) {
+    const float p = lum * (4.0f * 3.14159265f * (r * r));
+    return p > 0.0f && p < 3.0e38f ? p : 0.0f;
+}
+static float tri_area(const float* a, const float* b) {
+    const float cx = a[1] * b[2] - a[2] * b[1], cy = a[2] * b[0] - a[0] * b[2], cz = a[0] * b[1] - a[1] * b[0];
+    return 0.5f * sqrtf(cx * cx + cy * cy + cz * cz);
+}
+static float tri_power(float lum, float area) {
+    const float p = lum * area;
+    return p > 0.0f && p < 3.0e38f ? p : 0.0f;
+}
 
 po_scene* po_scene_create(const pt_scene_desc* d, const pt_bvh* flat, const pt_bvh* inst, const pt_bvh* meshes) {
     po_scene* s = (po_scene*)calloc(1, sizeof(po_scene));
@@ -111,6 +136,49 @@ po_scene* po_scene_create(const pt_scene_desc* d, const pt_bvh* flat, const pt_b
         for (i = 0; i < d->n_spheres; ++i)
             if (emits(&d->materials[d->spheres[i].material])) s->lights[s->n_lights++] = i;
     }
+    /* the extended list: the light spheres, then every emissive flat triangle of positive area */
+    {
+        uint32_t n, k;
+        float* power;
+        double total = 0, sum = 0, acc = 0;
+        s->tri_lights = (uint32_t*)calloc(d->n_triangles ? d->n_triangles : 1, sizeof(uint32_t));
+        s->tri_area = (float*)calloc(d->n_triangles ? d->n_triangles : 1, sizeof(float));
+        for (i = 0; i < d->n_triangles; ++i) {
+            const pt_triangle* t = &d->triangles[i];
+            float a;
+            if (!emits(&d->materials[t->material])) continue;
+            a = tri_area(t->e1, t->e2);
+            if (!(a > 0.0f) || !(a < 3.0e38f)) continue;
+            s->tri_area[s->n_tri_lights] = a;
+            s->tri_lights[s->n_tri_lights++] = i;
+        }
+        n = s->n_lights + s->n_tri_lights;
+        power = (float*)calloc(n ? n : 1, sizeof(float));
+        for (k = 0; k < s->n_lights; ++k) {
+            const pt_sphere* L = &d->spheres[s->lights[k]];
+            power[k] = sphere_power(light_lum(d->materials[L->material].emission), L->radius);
+        }
+        for (k = 0; k < s->n_tri_lights; ++k)
+            power[s->n_lights + k] = tri_power(light_lum(d->materials[d->triangles[s->tri_lights[k]].material].emission),
+                                               s->tri_area[k]);
+        s->light_cdf = (float*)calloc(n ? n : 1, sizeof(float));
+        if (n) {
+            for (k = 0; k < n; ++k) total += power[k];
+            if (total > 0) {
+                s->pick_uniform = (float)(0.5 / (double)n);
+                s->pick_power = (float)(0.5 / total);
+            } else {
+                s->pick_uniform = (float)(1.0 / (double)n);
+                s->pick_power = 0;
+            }
+            for (k = 0; k < n; ++k) sum += (double)(s->pick_uniform + s->pick_power * power[k]);
+            for (k = 0; k < n; ++k) {
+                acc += (double)(s->pick_uniform + s->pick_power * power[k]);
+                s->light_cdf[k] = k + 1 == n ? 1.0f : (float)(acc / sum);
+            }
+        }
+        free(power);
+    }
     return s;
 }
 
@@ -121,6 +189,9 @@ void po_scene_destroy(po_scene* s) {
     free(s->texels);
     free(s->mesh);
     free(s->lights);
+    free(s->tri_lights);
+    free(s->tri_area);
+    free(s->light_cdf);
     free(s);
 }
 
@@ -441,6 +512,11 @@ typedef struct {
     int front_face, sampled_light;
     uint32_t mat;
     float tex_u, tex_v;
+    /* extended light sampling: 1 a light sphere (lgeo = center, lw = radius),
+     * 2 an emissive flat triangle (lgeo = face normal, lw = area), else 0 */
+    int lkind;
+    v3 lgeo;
+    float lw;
 } rec_t;
 
 static void fill_sphere(const pt_sphere* s, v3 o, v3 d, float t, rec_t* r) {
@@ -484,11 +560,12 @@ static v3 sample_texture(const po_scene* s, uint32_t k, float u, float v) {
                scl(texel(s, k, x0 + 1, y0 + 1), fx * fy));
 }
 
-static int hit(const po_scene* s, v3 o, v3 d, float t_min, float t_max, rec_t* r, counts* cnt) {
+static int hit(const po_scene* s, v3 o, v3 d, float t_min, float t_max, rec_t* r, counts* cnt, int ext) {
     const pt_scene_desc* D = &s->d;
     hctx c;
     closest(s, o, d, t_min, &t_max, &c, cnt);
     r->sampled_light = 0;
+    r->lkind = 0;
     r->tex_u = 0;
     r->tex_v = 0;
     switch (c.kind) {
@@ -496,8 +573,26 @@ static int hit(const po_scene* s, v3 o, v3 d, float t_min, float t_max, rec_t* r
         case PT_HIT_SPHERE:
             fill_sphere(&D->spheres[c.index], o, d, t_max, r);
             r->sampled_light = D->sample_lights && emits(&D->materials[r->mat]);
+            if (ext && r->sampled_light) {
+                r->lkind = 1;
+                r->lgeo = ld3(D->spheres[c.index].center);
+                r->lw = D->spheres[c.index].radius;
+            }
             return 1;
-        case PT_HIT_TRIANGLE: fill_triangle(&D->triangles[c.index], o, d, t_max, c.u, c.v, r); return 1;
+        case PT_HIT_TRIANGLE: {
+            const pt_triangle* tr = &D->triangles[c.index];
+            fill_triangle(tr, o, d, t_max, c.u, c.v, r);
+            if (ext && D->sample_lights && emits(&D->materials[r->mat])) {
+                const float a = tri_area(tr->e1, tr->e2);
+                if (a > 0.0f && a < 3.0e38f) {
+                    r->sampled_light = 1;
+                    r->lkind = 2;
+                    r->lgeo = ld3(tr->face_normal);
+                    r->lw = a;
+                }
+            }
+            return 1;
+        }
         case PT_HIT_INSTANCE: {
             const pt_instance* in = &D->instances[c.index];
             v3 lo = aff_point(&in->to_object, o), ldir = aff_vector(&in->to_object, d);
@@ -743,11 +838,139 @@ static v3 direct_light(const po_scene* s, const rec_t* rec, const sampler_t* q, 
     return scl(ld3(s->d.materials[L->material].emission), cos_surface / (float)M_PI / pdf * (float)n);
 }
 
-/* ray_color<with_first> (:100-149) */
+/* ---- extended light sampling (PT_FLAG_NEE_EXTENDED; beyond the reference) ----------- */
+/* The density of metal's scattered direction (material.hpp:85-91: mirror r
+ * plus fuzz f times a point uniform in the unit ball) per unit solid angle at
+ * unit direction w: over the chord [t1, t2] of the ray t*w (t >= 0) through
+ * the ball of radius f about r, (t2^3 - t1^3) / (4 pi f^3). */
+static float metal_lobe_pdf(v3 rr, float f, v3 w) {
+    const float b = dot(w, rr), c = dot(rr, rr) - f * f;
+    const float disc = b * b - c;
+    float sq, t1, t2;
+    if (!(disc > 0)) return 0;
+    sq = sqrtf(disc);
+    t2 = b + sq;
+    if (!(t2 > 0)) return 0;
+    t1 = fmaxf(b - sq, 0.0f);
+    return (t2 * t2 * t2 - t1 * t1 * t1) / (4 * (float)M_PI * (f * f * f));
+}
+float po_metal_lobe_pdf(const float r[3], float f, const float w[3]) { return metal_lobe_pdf(ld3(r), f, ld3(w)); }
+
+static uint32_t pick_light_ext(const po_scene* s, float u) {
+    uint32_t lo = 0, hi = s->n_lights + s->n_tri_lights - 1;
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (u < s->light_cdf[mid]) hi = mid;
+        else lo = mid + 1;
+    }
+    return lo;
+}
+
+/* A light sample of the extended list from rec: the matte estimate
+ * (albedo / pi times the cosine; the albedo applied by the caller) or, with
+ * metal, the lobe density weighted against the scattered ray by the power
+ * heuristic. */
+static v3 direct_light_ext(const po_scene* s, const rec_t* rec, v3 mirror, float fuzz, int metal, const sampler_t* q,
+                           rng_t* r, uint64_t* rays, counts* cnt) {
+    const uint32_t k = pick_light_ext(s, rng_real(r));
+    v3 dir, le;
+    float cos_surface, pdf_solid, power, t_max, pdf, f, s1, s2;
+    int front = 1;
+    if (k < s->n_lights) {
+        const pt_sphere* L = &s->d.spheres[s->lights[k]];
+        v3 to_center, w, a, u, v, outward;
+        float dist2, r2, sin2_max, cos_max, omc, cos_t, sin_t, phi, t_light;
+        to_center = sub(ld3(L->center), rec->p);
+        dist2 = dot(to_center, to_center);
+        r2 = L->radius * L->radius;
+        if (dist2 <= r2) return mk(0, 0, 0);
+        sin2_max = r2 / dist2;
+        cos_max = sqrtf(1 - sin2_max);
+        omc = sin2_max / (1 + cos_max);
+        w = vdiv(to_center, sqrtf(dist2));
+        a = fabsf(w.x) > 0.9f ? mk(0, 1, 0) : mk(1, 0, 0);
+        u = normalize(cross(w, a));
+        v = cross(w, u);
+        sample_2d(q, r, 1, &s1, &s2);
+        cos_t = 1 - s1 * omc;
+        sin_t = sqrtf(fmaxf(0.0f, 1 - cos_t * cos_t));
+        phi = 2 * (float)M_PI * s2;
+        dir = add(add(scl(u, cosf(phi) * sin_t), scl(v, sinf(phi) * sin_t)), scl(w, cos_t));
+        cos_surface = dot(dir, rec->normal);
+        if (cos_surface <= 0) return mk(0, 0, 0);
+        t_light = INFINITY;
+        if (!sphere_hit(L, rec->p, dir, 0.001f, &t_light)) return mk(0, 0, 0);
+        ++*rays;
+        outward = scl(sub(add(rec->p, scl(dir, t_light)), ld3(L->center)), 1 / L->radius);
+        front = dot(dir, outward) < 0;
+        t_max = t_light * 0.9999f;
+        pdf_solid = 1 / (2 * (float)M_PI * omc);
+        le = ld3(s->d.materials[L->material].emission);
+        power = sphere_power(light_lum(s->d.materials[L->material].emission), L->radius);
+    } else {
+        const uint32_t ti = k - s->n_lights;
+        const pt_triangle* T = &s->d.triangles[s->tri_lights[ti]];
+        const float area = s->tri_area[ti];
+        float sq, dist2, dist, cos_l;
+        v3 y, dv;
+        sample_2d(q, r, 1, &s1, &s2);
+        sq = sqrtf(s1);
+        y = add(add(ld3(T->p0), scl(ld3(T->e1), 1 - sq)), scl(ld3(T->e2), s2 * sq));
+        dv = sub(y, rec->p);
+        dist2 = dot(dv, dv);
+        if (!(dist2 > 0)) return mk(0, 0, 0);
+        dist = sqrtf(dist2);
+        dir = scl(dv, 1.0f / dist);
+        cos_l = -dot(dir, ld3(T->face_normal));
+        if (!(cos_l > 0)) return mk(0, 0, 0);
+        cos_surface = dot(dir, rec->normal);
+        if (cos_surface <= 0) return mk(0, 0, 0);
+        ++*rays;
+        t_max = dist * 0.9999f;
+        pdf_solid = dist2 / (area * cos_l);
+        le = ld3(s->d.materials[T->material].emission);
+        power = tri_power(light_lum(s->d.materials[T->material].emission), area);
+    }
+    pdf = (s->pick_uniform + s->pick_power * power) * pdf_solid;
+    if (!(pdf > 0) || !(pdf < 3.0e38f)) return mk(0, 0, 0);
+    if (metal) {
+        const float pb = metal_lobe_pdf(mirror, fuzz, dir), qq = pb / pdf;
+        f = qq * (1 / (1 + qq * qq));
+    } else {
+        f = cos_surface / (float)M_PI / pdf;
+    }
+    if (!front || !(f > 0)) return mk(0, 0, 0);
+    if (occluded(s, rec->p, dir, 0.001f, t_max, cnt)) return mk(0, 0, 0);
+    return scl(le, f);
+}
+
+/* The extended light-sampling density of direction d from x that hit the light in rec. */
+static float light_pdf_at_hit(const po_scene* s, const rec_t* rec, v3 x, v3 d, const float* em) {
+    float pdf_solid, power;
+    const float lum = light_lum(em);
+    if (rec->lkind == 1) {
+        const v3 to_center = sub(rec->lgeo, x);
+        const float dist2 = dot(to_center, to_center), r2 = rec->lw * rec->lw;
+        float sin2_max;
+        if (dist2 <= r2) return 0;
+        sin2_max = r2 / dist2;
+        pdf_solid = 1 / (2 * (float)M_PI * (sin2_max / (1 + sqrtf(1 - sin2_max))));
+        power = sphere_power(lum, rec->lw);
+    } else {
+        const float dl = sqrtf(dot(d, d)), dist = rec->t * dl;
+        const float cos_l = fabsf(dot(d, rec->lgeo)) / dl;
+        pdf_solid = dist * dist / (rec->lw * cos_l);
+        power = tri_power(lum, rec->lw);
+    }
+    return (s->pick_uniform + s->pick_power * power) * pdf_solid;
+}
+
+/* ray_color<with_first> (:100-149); ext: the extended light sampling. */
 static v3 ray_color(const po_scene* s, v3 o, v3 d, int depth, sampler_t* q, rng_t* r, v3* f_albedo, v3* f_normal,
-                    uint64_t* rays, counts* cnt) {
+                    uint64_t* rays, counts* cnt, int ext) {
     v3 tp = mk(1, 1, 1), rad = mk(0, 0, 0);
     int sampled = 0, bounce;
+    float mis_pdf = 0;
     for (bounce = 0; bounce < depth; ++bounce) {
         rec_t rec;
         const pt_material* m;
@@ -755,7 +978,7 @@ static v3 ray_color(const po_scene* s, v3 o, v3 d, int depth, sampler_t* q, rng_
         int scatters;
         ++*rays;
         q->base = 1 + 2 * bounce;
-        if (!hit(s, o, d, 0.001f, 1000, &rec, cnt)) {
+        if (!hit(s, o, d, 0.001f, 1000, &rec, cnt, ext)) {
             if (bounce == 0) {
                 *f_albedo = mk(1, 1, 1);
                 *f_normal = mk(0, 0, 0);
@@ -763,7 +986,14 @@ static v3 ray_color(const po_scene* s, v3 o, v3 d, int depth, sampler_t* q, rng_
             return add(rad, mul(tp, background(s, d)));
         }
         m = &s->d.materials[rec.mat];
-        if (rec.front_face && !(sampled && rec.sampled_light)) rad = add(rad, mul(tp, ld3(m->emission)));
+        if (rec.front_face && !(sampled && rec.sampled_light)) {
+            if (ext && mis_pdf > 0 && rec.sampled_light) {
+                const float qq = light_pdf_at_hit(s, &rec, o, d, m->emission) / mis_pdf;
+                rad = add(rad, mul(tp, scl(ld3(m->emission), 1 / (1 + qq * qq))));
+            } else {
+                rad = add(rad, mul(tp, ld3(m->emission)));
+            }
+        }
         scatters = scatter(m, d, &rec, q, r, &att, &dir);
         /* lambertian: albedo * texture->sample(tex_u, tex_v) (material.hpp:72) */
         if (m->type == PT_MAT_LAMBERTIAN && m->texture > 0) att = mul(att, sample_texture(s, m->texture - 1, rec.tex_u, rec.tex_v));
@@ -771,9 +1001,23 @@ static v3 ray_color(const po_scene* s, v3 o, v3 d, int depth, sampler_t* q, rng_
             *f_albedo = scatters && m->type != PT_MAT_DIELECTRIC ? att : mk(1, 1, 1);
             *f_normal = rec.normal;
         }
-        if (!scatters) return rad;
-        sampled = m->type == PT_MAT_LAMBERTIAN && s->d.sample_lights && s->n_lights > 0 && bounce + 1 < depth;
-        if (sampled) rad = add(rad, mul(mul(tp, att), direct_light(s, &rec, q, r, rays, cnt)));
+        if (ext) {
+            const int can = s->d.sample_lights && s->n_lights + s->n_tri_lights > 0 && bounce + 1 < depth;
+            const float fuzz = m->fuzz < 1 ? m->fuzz : 1;
+            mis_pdf = 0;
+            if (m->type == PT_MAT_METAL && fuzz > 1e-3f && can) {
+                const v3 mirror = reflect(normalize(d), rec.normal);
+                rad = add(rad, mul(mul(tp, att), direct_light_ext(s, &rec, mirror, fuzz, 1, q, r, rays, cnt)));
+                if (scatters) mis_pdf = metal_lobe_pdf(mirror, fuzz, normalize(dir));
+            }
+            if (!scatters) return rad;
+            sampled = m->type == PT_MAT_LAMBERTIAN && can;
+            if (sampled) rad = add(rad, mul(mul(tp, att), direct_light_ext(s, &rec, mk(0, 0, 0), 0, 0, q, r, rays, cnt)));
+        } else {
+            if (!scatters) return rad;
+            sampled = m->type == PT_MAT_LAMBERTIAN && s->d.sample_lights && s->n_lights > 0 && bounce + 1 < depth;
+            if (sampled) rad = add(rad, mul(mul(tp, att), direct_light(s, &rec, q, r, rays, cnt)));
+        }
         tp = mul(tp, att);
         o = rec.p;
         d = dir;
@@ -797,9 +1041,9 @@ static float luminance(v3 c) { return 0.2126f * c.x + 0.7152f * c.y + 0.0722f * 
  * per-sample states (PT_RNG_SNAPSHOT), 2 = the reference's own per-row stream
  * (seed_row, renderer.hpp:349-351). render_row_impl (:366-409).
  */
-void po_render(const po_scene* s, const pt_camera* cam, int W, int H, int spp, int depth, uint64_t seed,
-               int first_sample, int rng_mode, const uint64_t* states, int row0, int rows, float* out, float* aux,
-               uint64_t* rays_out, uint64_t counts_out[5]) {
+void po_render_flags(const po_scene* s, const pt_camera* cam, int W, int H, int spp, int depth, uint64_t seed,
+                     int first_sample, int rng_mode, const uint64_t* states, int row0, int rows, float* out,
+                     float* aux, uint64_t* rays_out, uint64_t counts_out[5], int flags) {
     v3 origin = ld3(cam->origin), llc = ld3(cam->lower_left), hz = ld3(cam->horizontal), vt = ld3(cam->vertical);
     float scale = 1.0f / spp;
     uint64_t rays = 0;
@@ -828,7 +1072,8 @@ void po_render(const po_scene* s, const pt_camera* cam, int W, int H, int spp, i
                 dir = sub(add(add(llc, scl(hz, u)), scl(vt, v)), origin);
                 if (rng_mode == 0) rng_seed(&r, po_sample_stream_seed(seed, i, j, idx));
                 if (rng_mode == 1) memcpy(r.s, states + 4 * (((size_t)j * W + i) * spp + k), 32);
-                c = ray_color(s, origin, dir, depth, &q, &r, &fa, &fn, &rays, counts_out ? &cnt : NULL);
+                c = ray_color(s, origin, dir, depth, &q, &r, &fa, &fn, &rays, counts_out ? &cnt : NULL,
+                              (flags & PT_FLAG_NEE_EXTENDED) != 0);
                 pc = add(pc, c);
                 alb = add(alb, fa);
                 nor = add(nor, fn);
@@ -857,6 +1102,13 @@ void po_render(const po_scene* s, const pt_camera* cam, int W, int H, int spp, i
         counts_out[3] = cnt.spheres;
         counts_out[4] = cnt.insts;
     }
+}
+
+void po_render(const po_scene* s, const pt_camera* cam, int W, int H, int spp, int depth, uint64_t seed,
+               int first_sample, int rng_mode, const uint64_t* states, int row0, int rows, float* out, float* aux,
+               uint64_t* rays_out, uint64_t counts_out[5]) {
+    po_render_flags(s, cam, W, H, spp, depth, seed, first_sample, rng_mode, states, row0, rows, out, aux, rays_out,
+                    counts_out, 0);
 }
 
 /* Ray queries: geometry::hit's choice and geometry::occluded, per ray. */

@@ -32,6 +32,7 @@ PT_MAT_LAMBERTIAN, PT_MAT_METAL, PT_MAT_DIELECTRIC, PT_MAT_DIFFUSE_LIGHT = 0, 1,
 PT_NO_MATERIAL = 0xFFFFFFFF
 PT_MODE_AUTO, PT_MODE_MEGAKERNEL, PT_MODE_WAVEFRONT = 0, 1, 2
 PT_RNG_SAMPLE, PT_RNG_SNAPSHOT = 0, 1
+PT_FLAG_NEE_EXTENDED = 1
 PT_HIT_NONE, PT_HIT_LARGE, PT_HIT_SPHERE, PT_HIT_TRIANGLE, PT_HIT_INSTANCE = 0, 1, 2, 3, 4
 
 PT_GEN_REF_MATERIALS = 0
@@ -42,6 +43,7 @@ PT_GEN_ROOM_MESH = 11
 PT_GEN_INSTANCES = 12
 PT_GEN_BATCH_SCENE = 13
 PT_GEN_TEXTURED = 14
+PT_GEN_MESH_LIGHT = 15
 
 PT_ATROUS_NOALLOC_MAX_PIXELS = 262144  # the built-in scratch of pt_denoise_atrous_device_noalloc
 
@@ -113,7 +115,7 @@ class pt_camera(C.Structure):
 class pt_settings(C.Structure):
     _fields_ = [("width", C.c_int32), ("height", C.c_int32), ("spp", C.c_int32), ("max_bounces", C.c_int32),
                 ("seed", C.c_uint64), ("first_sample", C.c_int32), ("mode", C.c_int32), ("rng", C.c_int32),
-                ("reserved", C.c_int32), ("rng_states", C.POINTER(C.c_uint64))]
+                ("flags", C.c_int32), ("rng_states", C.POINTER(C.c_uint64))]
 
 
 class pt_hit(C.Structure):

@@ -157,9 +157,10 @@ class Scene:
     # -- rendering --
     def render(self, cam, width: int, height: int, spp: int, max_bounces: int = 10, seed: int = 1,
                first_sample: int = 0, mode: int = abi.PT_MODE_AUTO, rng: int = abi.PT_RNG_SAMPLE,
-               states: Optional[np.ndarray] = None, aux: bool = False):
-        """A frame with host buffers. Returns (image H x W x 3 top row first, aux H x W x 7 or None, rays)."""
-        st = self.settings(width, height, spp, max_bounces, seed, first_sample, mode, rng, states)
+               states: Optional[np.ndarray] = None, aux: bool = False, flags: int = 0):
+        """A frame with host buffers. Returns (image H x W x 3 top row first, aux H x W x 7 or None, rays).
+        flags: PT_FLAG_* (PT_FLAG_NEE_EXTENDED: light sampling toward emissive triangles and from rough metal)."""
+        st = self.settings(width, height, spp, max_bounces, seed, first_sample, mode, rng, states, flags=flags)
         out = np.empty((height, width, 3), np.float32)
         ax = np.empty((height, width, 7), np.float32) if aux else None
         rays = C.c_uint64()
@@ -168,9 +169,9 @@ class Scene:
 
     @staticmethod
     def settings(width, height, spp, max_bounces=10, seed=1, first_sample=0, mode=abi.PT_MODE_AUTO,
-                 rng=abi.PT_RNG_SAMPLE, states=None, states_ptr=None) -> abi.pt_settings:
+                 rng=abi.PT_RNG_SAMPLE, states=None, states_ptr=None, flags=0) -> abi.pt_settings:
         st = abi.pt_settings(width=width, height=height, spp=spp, max_bounces=max_bounces, seed=seed,
-                             first_sample=first_sample, mode=mode, rng=rng)
+                             first_sample=first_sample, mode=mode, rng=rng, flags=flags)
         if states is not None:
             states = np.ascontiguousarray(states, np.uint64)
             st.rng_states = states.ctypes.data_as(C.POINTER(C.c_uint64))

@@ -71,7 +71,7 @@ struct pt_scene {
     cudaStream_t stream = nullptr;
     Scratch out, aux, states, in_rays, out_hits, counts, wave, sum;
     uint32_t* host_counts = nullptr;  // pinned, for the wavefront queue read-back
-    int blocks_per_sm[4] = {0, 0, 0, 0};
+    int blocks_per_sm[6] = {0, 0, 0, 0, 0, 0};  // megakernel forms: aux, snapshot; extended light sampling
 };
 
 namespace {
@@ -122,6 +122,11 @@ pt_status check_settings(const pt_settings* st) {
         return fail(PT_ERR_INVALID_ARG, "settings: PT_RNG_SNAPSHOT needs rng_states");
     if (st->mode < PT_MODE_AUTO || st->mode > PT_MODE_WAVEFRONT)
         return fail(PT_ERR_INVALID_ARG, "settings: unknown mode");
+    if (st->flags & ~int32_t(PT_FLAG_NEE_EXTENDED)) return fail(PT_ERR_INVALID_ARG, "settings: unknown flags");
+    if ((st->flags & PT_FLAG_NEE_EXTENDED) && st->rng == PT_RNG_SNAPSHOT)
+        return fail(PT_ERR_UNSUPPORTED, "settings: PT_FLAG_NEE_EXTENDED needs PT_RNG_SAMPLE streams");
+    if ((st->flags & PT_FLAG_NEE_EXTENDED) && st->mode == PT_MODE_WAVEFRONT)
+        return fail(PT_ERR_UNSUPPORTED, "settings: PT_FLAG_NEE_EXTENDED renders with the megakernel");
     return PT_OK;
 }
 
@@ -139,6 +144,7 @@ PtRenderParams make_params(const pt_camera* cam, const pt_settings* st) {
     p.seed = st->seed;
     p.first_sample = st->first_sample;
     p.rng_mode = st->rng;
+    p.nee_ext = (st->flags & PT_FLAG_NEE_EXTENDED) ? 1 : 0;
     p.states = st->rng_states;
     p.row0 = 0;
     p.rows = st->height;
@@ -161,12 +167,12 @@ pt_status launch_render(pt_scene* s, PtRenderParams& p, int mode, cudaStream_t s
         return PT_OK;
     }
     if (cudaError_t e = cudaMemsetAsync(s->work, 0, sizeof(unsigned int), stream)) return cuda_fail(e, "render");
-    const int variant = (p.aux ? 1 : 0) + (p.rng_mode == PT_RNG_SNAPSHOT ? 2 : 0);
+    const int variant = p.nee_ext ? 4 + (p.aux ? 1 : 0) : (p.aux ? 1 : 0) + (p.rng_mode == PT_RNG_SNAPSHOT ? 2 : 0);
     PtLaunchShape shape;
     shape.threads = 128;
     if (!s->blocks_per_sm[variant])
         s->blocks_per_sm[variant] = pt_megakernel_blocks_per_sm(s->dev, shape.threads, p.aux != nullptr,
-                                                                p.rng_mode == PT_RNG_SNAPSHOT);
+                                                                p.rng_mode == PT_RNG_SNAPSHOT, p.nee_ext != 0);
     shape.blocks = s->sms * s->blocks_per_sm[variant];
     p.work = s->work;
     if (cudaError_t e = pt_launch_megakernel(s->dev, p, shape, stream)) return cuda_fail(e, "megakernel launch");
@@ -257,7 +263,9 @@ pt_status pt_scene_create(const pt_scene_desc* desc, pt_scene** out) {
                          align256(A.sph.size() * sizeof(PtShadeSphere)) + align256(A.tri.size() * sizeof(PtShadeTri)) +
                          align256(A.inst.size() * sizeof(PtShadeInst)) + align256(A.mat.size() * sizeof(PtMaterial)) +
                          align256(A.lights.size() * sizeof(PtLight)) + align256(A.tri_uv.size() * 4) +
-                         align256(A.tex.size() * sizeof(int4)) + align256(A.texels.size() * 4) + 3 * 256;
+                         align256(A.tex.size() * sizeof(int4)) + align256(A.texels.size() * 4) +
+                         align256(A.tri_lights.size() * sizeof(PtTriLight)) + align256(A.light_cdf.size() * 4) +
+                         3 * 256;
     cudaError_t err = cudaMalloc(&s->arena, bytes);
     if (err != cudaSuccess) {
         delete s;
@@ -277,6 +285,8 @@ pt_status pt_scene_create(const pt_scene_desc* desc, pt_scene** out) {
     D.inst = upload(base, off, A.inst, err);
     D.mat = upload(base, off, A.mat, err);
     D.lights = upload(base, off, A.lights, err);
+    D.tri_lights = upload(base, off, A.tri_lights, err);
+    D.light_cdf = upload(base, off, A.light_cdf, err);
     D.tri_uv = upload(base, off, A.tri_uv, err);
     D.tex = upload(base, off, A.tex, err);
     D.texels = upload(base, off, A.texels, err);
@@ -302,6 +312,9 @@ pt_status pt_scene_create(const pt_scene_desc* desc, pt_scene** out) {
     D.n_instances = A.n_instances;
     D.n_large = uint32_t(A.large.size());
     D.n_lights = uint32_t(A.lights.size());
+    D.n_tri_lights = uint32_t(A.tri_lights.size());
+    D.pick_uniform = A.pick_uniform;
+    D.pick_power = A.pick_power;
     D.n_spheres = A.n_spheres;
     D.sky = A.sky;
     D.sample_lights = A.sample_lights;

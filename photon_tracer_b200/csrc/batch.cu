@@ -34,6 +34,13 @@ __device__ __forceinline__ unsigned long long global_ns() {
 #define PT_BATCH_MIN_BLOCKS128 4
 #endif
 
+// Traversal-stack entries per lane in shared memory: 0, as measured best for
+// the single-scene megakernel this kernel follows (at most 48 KB of static
+// shared memory per block, so at most 12 entries at 256 threads).
+#ifndef PT_BATCH_SH_STACK
+#define PT_BATCH_SH_STACK 0
+#endif
+
 #ifndef PT_BATCH_ONE_QUERY
 #define PT_BATCH_ONE_QUERY 1
 #endif
@@ -41,7 +48,8 @@ __device__ __forceinline__ unsigned long long global_ns() {
 template <int THREADS, int TREES, bool TEX>
 __global__ void __launch_bounds__(THREADS, PT_BATCH_MIN_BLOCKS128 * 128 / THREADS)
     batch_megakernel(PtSceneDev S0, PtBatchLaunch B) {
-    StackEntry stack[PT_STACK_MAX];
+    // the stack in local memory, as the single-scene megakernel keeps it
+    PT_TRAV_STACK_N(stack, THREADS, PT_BATCH_SH_STACK);
     const int lane = threadIdx.x & 31;
     if (threadIdx.x == 0) atomicMin(B.start_ns, global_ns());
 
@@ -136,13 +144,14 @@ __global__ void __launch_bounds__(THREADS, PT_BATCH_MIN_BLOCKS128 * 128 / THREAD
                 path.rad = mk(0, 0, 0);
                 path.bounce = 0;
                 path.sampled = false;
+                path.mis_pdf = 0;
                 rng.seed(sample_stream_seed(seed, pi, pj, idx));
                 in_path = true;
             }
         }
 
         if constexpr (ONE_QUERY) {
-            if (in_path && query_trip<false, TEX>(S, path, depth, smp, rng, first, pend, shadow_pending,
+            if (in_path && query_trip<false, TEX, false>(S, path, depth, smp, rng, first, pend, shadow_pending,
                                                   done_after_shadow, stack, rays, overflow)) {
                 acc = acc + path.rad;
                 in_path = false;
@@ -160,10 +169,10 @@ __global__ void __launch_bounds__(THREADS, PT_BATCH_MIN_BLOCKS128 * 128 / THREAD
                 h.kind = PT_HIT_NONE;
             }
             const bool hit = h.kind != PT_HIT_NONE;
-            if (hit) fill<TEX>(S, h, path.o, path.d, t, rec);
+            if (hit) fill<TEX, false>(S, h, path.o, path.d, t, rec);
             bool nee;
             Shadow sh;
-            const int step = shade<false, TEX>(S, path, hit, rec, depth, smp, rng, first, nee, sh, rays);
+            const int step = shade<false, TEX, false>(S, path, hit, rec, depth, smp, rng, first, nee, sh, rays);
             if (nee) {
                 bool ovf = false;
                 if (!occluded<false, TREES>(S, sh.o, sh.d, 0.001f, sh.t_max, stack, cnt, &ovf)) path.rad = path.rad + sh.value;

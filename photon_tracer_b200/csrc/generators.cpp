@@ -428,6 +428,42 @@ void room_mesh_scene(SceneBuilder& b, uint64_t seed, int subdiv) {
     b.g->triangles.insert(b.g->triangles.end(), tris.begin(), tris.end());
 }
 
+// The reference's room lit by emissive meshes instead of its lamp sphere (no
+// counterpart in the reference, whose light sampling covers spheres only,
+// README.md:453-456): a lamp of 80 emissive triangles (a once-subdivided
+// icosphere, flat-shaded, faces outward) where the sphere lamp hangs, an
+// emissive ceiling panel (2 triangles facing down) and a small light sphere,
+// over glass, rough metal (fuzz 0.25), a mirror (fuzz 0) and matte spheres:
+// the scene of the extended light-sampling tests.
+void mesh_light_room_scene(SceneBuilder& b) {
+    b.g->desc.sky = 0;
+    const uint32_t white = b.lambertian(p3(0.73, 0.73, 0.73));
+    const uint32_t red = b.lambertian(p3(0.65, 0.05, 0.05));
+    const uint32_t green = b.lambertian(p3(0.12, 0.45, 0.15));
+    const double x0 = -1.75, x1 = 1.75, y0 = -1, y1 = 1, z0 = -3.5, z1 = 0.5;
+    b.quad(p3(x0, y0, z1), p3(x1 - x0, 0, 0), p3(0, 0, z0 - z1), white);  // floor
+    b.quad(p3(x0, y1, z1), p3(x1 - x0, 0, 0), p3(0, 0, z0 - z1), white);  // ceiling
+    b.quad(p3(x0, y0, z0), p3(x1 - x0, 0, 0), p3(0, y1 - y0, 0), white);  // back
+    b.quad(p3(x0, y0, z1), p3(x1 - x0, 0, 0), p3(0, y1 - y0, 0), white);  // front
+    b.quad(p3(x0, y0, z1), p3(0, 0, z0 - z1), p3(0, y1 - y0, 0), red);    // left
+    b.quad(p3(x1, y0, z1), p3(0, 0, z0 - z1), p3(0, y1 - y0, 0), green);  // right
+    const uint32_t lamp = b.light(p3(30, 27, 22));
+    const Mesh ico = icosphere(1);
+    const double lc[3] = {0, 0.72, -2.0}, lr = 0.14;
+    for (const auto& f : ico.f) {
+        V3 c[3];
+        for (int k = 0; k < 3; ++k)
+            c[k] = p3(lc[0] + lr * ico.v[f[k]][0], lc[1] + lr * ico.v[f[k]][1], lc[2] + lr * ico.v[f[k]][2]);
+        b.g->triangles.push_back(make_triangle(c[0], c[1], c[2], lamp));
+    }
+    b.quad(p3(-0.3, 0.999, -1.2), p3(0, 0, -0.6), p3(0.6, 0, 0), b.light(p3(3, 3, 3)));  // panel, facing down
+    b.sphere(p3(0.9, 0.5, -2.6), 0.05f, b.light(p3(40, 40, 40)));
+    b.sphere(p3(-0.8, -0.55, -2.3), 0.45f, b.dielectric(1.5f));
+    b.sphere(p3(0.85, -0.6, -1.8), 0.4f, b.metal(p3(0.9, 0.8, 0.7), 0.25f));
+    b.sphere(p3(0.3, -0.8, -1.3), 0.2f, b.metal(p3(0.9, 0.9, 0.9), 0.0f));
+    b.sphere(p3(0.15, -0.75, -2.9), 0.25f, b.lambertian(p3(0.1, 0.2, 0.5)));
+}
+
 // 10,000 instances of a displaced icosphere (20,480), a (3,7) torus knot
 // (50,000) and a 256x256 heightfield (131,072) over a 200x200 area, ground
 // sphere r=1000, 8 light spheres r=3 emission 8 at height 40.
@@ -658,6 +694,11 @@ pt_status pt_generate(pt_gen_params* params, pt_generated** out) {
             instances_scene(b, params->seed, params->param > 0 ? params->param : 10000);
             store(from, p3(0, 35, 140)); store(at, p3(0, 0, 0)); vfov = 45.0;
             width = 1920; height = 1080; spp = 32;
+            break;
+        case PT_GEN_MESH_LIGHT:
+            mesh_light_room_scene(b);
+            store(from, p3(0, 0, 0.3)); store(at, p3(0, -0.15, -3.0)); vfov = 62.0;
+            width = 960; height = 540; spp = 200;
             break;
         case PT_GEN_TEXTURED:
             textured_scene(b, params->seed);

@@ -17,6 +17,7 @@ struct PtRenderParams {
     uint64_t seed;
     int first_sample;
     int rng_mode;               // PT_RNG_*
+    int nee_ext;                // PT_FLAG_NEE_EXTENDED (megakernel, production streams)
     const uint64_t* states;     // PT_RNG_SNAPSHOT: per (pixel, sample) xoshiro state
     int row0, rows, flip;
     float* out;                 // 3 floats per pixel
@@ -34,7 +35,7 @@ struct PtLaunchShape {
 // renders its pixel's samples one path after another.
 cudaError_t pt_launch_megakernel(const PtSceneDev& scene, const PtRenderParams& p, const PtLaunchShape& shape,
                                  cudaStream_t stream);
-int pt_megakernel_blocks_per_sm(const PtSceneDev& scene, int threads, bool aux, bool snapshot);
+int pt_megakernel_blocks_per_sm(const PtSceneDev& scene, int threads, bool aux, bool snapshot, bool ext);
 
 // Ray queries: closest hit (pt_hit records), any hit (bytes), and traversal
 // work counters (5 x u64, added to).

@@ -51,10 +51,24 @@ constexpr int kTileW = 8, kTileH = 4;
 #define PT_MEGA_ONE_QUERY 1
 #endif
 
-template <bool AUX, bool SNAP, int TREES, bool TEX>
+// Traversal-stack entries per lane in shared memory (the rest in its local
+// array). Measured on the 1024x1024 room frame, the 1080p random-spheres
+// frame and the 10,000-instance frame (identical images): 0 is fastest; 2, 4
+// and 8 entries lost 1-3%, 1-5% and 1-6% (the kernel already keeps 15 KB of
+// path state per block in shared memory; a stack on top leaves the SM's L1
+// data cache 60 KB smaller for node and primitive fetches), 16 lost 14%.
+// The wavefront stages and ray-query kernels, with no other shared state,
+// gain from it and use PT_SH_STACK.
+#ifndef PT_MEGA_SH_STACK
+#define PT_MEGA_SH_STACK 0
+#endif
+
+// EXT: the extended light sampling of PT_FLAG_NEE_EXTENDED (production
+// streams only); false compiles exactly the reference's estimator.
+template <bool AUX, bool SNAP, int TREES, bool TEX, bool EXT>
 __global__ void __launch_bounds__(128, PT_MEGA_MIN_BLOCKS) megakernel(PtSceneDev S, PtRenderParams P, uint32_t tiles_x,
                                                   uint32_t total_items) {
-    StackEntry stack[PT_STACK_MAX];
+    PT_TRAV_STACK_N(stack, 128, PT_MEGA_SH_STACK);
     const int lane = threadIdx.x & 31;
     const Cam cam = {mk(P.cam.origin[0], P.cam.origin[1], P.cam.origin[2]),
                      mk(P.cam.llc[0], P.cam.llc[1], P.cam.llc[2]),
@@ -145,6 +159,7 @@ __global__ void __launch_bounds__(128, PT_MEGA_MIN_BLOCKS) megakernel(PtSceneDev
                 path.rad = mk(0, 0, 0);
                 path.bounce = 0;
                 path.sampled = false;
+                path.mis_pdf = 0;
                 first = {mk(0, 0, 0), mk(0, 0, 0)};
                 if (SNAP) {
                     const uint64_t* st = P.states + 4 * ((size_t(pj) * P.width + pi) * P.spp + s);
@@ -160,7 +175,7 @@ __global__ void __launch_bounds__(128, PT_MEGA_MIN_BLOCKS) megakernel(PtSceneDev
         }
 
         if constexpr (ONE_QUERY) {
-            if (in_path && query_trip<AUX, TEX>(S, path, P.depth, smp, rng, first, pend, shadow_pending,
+            if (in_path && query_trip<AUX, TEX, EXT>(S, path, P.depth, smp, rng, first, pend, shadow_pending,
                                                 done_after_shadow, stack, rays, overflow)) {
                 acc = acc + path.rad;
                 if (AUX) {
@@ -186,10 +201,10 @@ __global__ void __launch_bounds__(128, PT_MEGA_MIN_BLOCKS) megakernel(PtSceneDev
                 h.kind = PT_HIT_NONE;
             }
             const bool hit = h.kind != PT_HIT_NONE;
-            if (hit) fill<TEX>(S, h, path.o, path.d, t, rec);
+            if (hit) fill<TEX, EXT>(S, h, path.o, path.d, t, rec);
             bool nee;
             Shadow sh;
-            const int step = shade<AUX, TEX>(S, path, hit, rec, P.depth, smp, rng, first, nee, sh, rays);
+            const int step = shade<AUX, TEX, EXT>(S, path, hit, rec, P.depth, smp, rng, first, nee, sh, rays);
             if (nee) {
                 bool ovf = false;
                 if (!occluded<false, TREES>(S, sh.o, sh.d, 0.001f, sh.t_max, stack, cnt, &ovf))
@@ -237,12 +252,12 @@ __global__ void __launch_bounds__(128, PT_MEGA_MIN_BLOCKS) megakernel(PtSceneDev
     if (__any_sync(0xffffffffu, overflow) && lane == 0) atomicOr(S.status, PT_DEV_ERR_STACK);
 }
 
-template <bool AUX, bool SNAP, int TREES, bool TEX>
+template <bool AUX, bool SNAP, int TREES, bool TEX, bool EXT>
 cudaError_t launch(const PtSceneDev& S, const PtRenderParams& p, const PtLaunchShape& shape, cudaStream_t stream) {
     const uint32_t tiles_x = uint32_t((p.width + kTileW - 1) / kTileW);
     const uint32_t tiles_y = uint32_t((p.rows + kTileH - 1) / kTileH);
     const uint32_t total = tiles_x * tiles_y * 32u;
-    megakernel<AUX, SNAP, TREES, TEX><<<shape.blocks, shape.threads, 0, stream>>>(S, p, tiles_x, total);
+    megakernel<AUX, SNAP, TREES, TEX, EXT><<<shape.blocks, shape.threads, 0, stream>>>(S, p, tiles_x, total);
     return cudaGetLastError();
 }
 
@@ -250,19 +265,24 @@ template <int TREES, bool TEX>
 cudaError_t launch_form(const PtSceneDev& S, const PtRenderParams& p, const PtLaunchShape& shape,
                         cudaStream_t stream) {
     const bool aux = p.aux != nullptr, snap = p.rng_mode == 1;
+    if (p.nee_ext)  // production streams only (the host refuses it with snapshots)
+        return aux ? launch<true, false, TREES, TEX, true>(S, p, shape, stream)
+                   : launch<false, false, TREES, TEX, true>(S, p, shape, stream);
     if (aux)
-        return snap ? launch<true, true, TREES, TEX>(S, p, shape, stream)
-                    : launch<true, false, TREES, TEX>(S, p, shape, stream);
-    return snap ? launch<false, true, TREES, TEX>(S, p, shape, stream)
-                : launch<false, false, TREES, TEX>(S, p, shape, stream);
+        return snap ? launch<true, true, TREES, TEX, false>(S, p, shape, stream)
+                    : launch<true, false, TREES, TEX, false>(S, p, shape, stream);
+    return snap ? launch<false, true, TREES, TEX, false>(S, p, shape, stream)
+                : launch<false, false, TREES, TEX, false>(S, p, shape, stream);
 }
 
 template <int TREES, bool TEX>
-int occupancy(int threads, bool aux, bool snap) {
-    const void* fn = aux ? (snap ? reinterpret_cast<const void*>(megakernel<true, true, TREES, TEX>)
-                                 : reinterpret_cast<const void*>(megakernel<true, false, TREES, TEX>))
-                         : (snap ? reinterpret_cast<const void*>(megakernel<false, true, TREES, TEX>)
-                                 : reinterpret_cast<const void*>(megakernel<false, false, TREES, TEX>));
+int occupancy(int threads, bool aux, bool snap, bool ext) {
+    const void* fn = ext ? (aux ? reinterpret_cast<const void*>(megakernel<true, false, TREES, TEX, true>)
+                                : reinterpret_cast<const void*>(megakernel<false, false, TREES, TEX, true>))
+                   : aux ? (snap ? reinterpret_cast<const void*>(megakernel<true, true, TREES, TEX, false>)
+                                 : reinterpret_cast<const void*>(megakernel<true, false, TREES, TEX, false>))
+                         : (snap ? reinterpret_cast<const void*>(megakernel<false, true, TREES, TEX, false>)
+                                 : reinterpret_cast<const void*>(megakernel<false, false, TREES, TEX, false>));
     return pt_resident_blocks(fn, threads, 0);
 }
 
@@ -284,12 +304,12 @@ cudaError_t pt_launch_megakernel(const PtSceneDev& S, const PtRenderParams& p, c
                           : launch_form<PT_TREES_EACH, false>(S, p, shape, stream);
 }
 
-int pt_megakernel_blocks_per_sm(const PtSceneDev& S, int threads, bool aux, bool snapshot) {
+int pt_megakernel_blocks_per_sm(const PtSceneDev& S, int threads, bool aux, bool snapshot, bool ext) {
     if (S.has_textures)
-        return one_loop(S)   ? occupancy<PT_TREES_ONE, true>(threads, aux, snapshot)
-               : flat_only(S) ? occupancy<PT_TREES_FLAT, true>(threads, aux, snapshot)
-                              : occupancy<PT_TREES_EACH, true>(threads, aux, snapshot);
-    return one_loop(S)   ? occupancy<PT_TREES_ONE, false>(threads, aux, snapshot)
-           : flat_only(S) ? occupancy<PT_TREES_FLAT, false>(threads, aux, snapshot)
-                          : occupancy<PT_TREES_EACH, false>(threads, aux, snapshot);
+        return one_loop(S)   ? occupancy<PT_TREES_ONE, true>(threads, aux, snapshot, ext)
+               : flat_only(S) ? occupancy<PT_TREES_FLAT, true>(threads, aux, snapshot, ext)
+                              : occupancy<PT_TREES_EACH, true>(threads, aux, snapshot, ext);
+    return one_loop(S)   ? occupancy<PT_TREES_ONE, false>(threads, aux, snapshot, ext)
+           : flat_only(S) ? occupancy<PT_TREES_FLAT, false>(threads, aux, snapshot, ext)
+                          : occupancy<PT_TREES_EACH, false>(threads, aux, snapshot, ext);
 }

@@ -19,6 +19,7 @@
 //
 // and shading data indexed by original numbers (read once per hit).
 #pragma once
+#include <math.h>
 #include <stdint.h>
 
 #define PT_LEAF_HAS_SPHERE 0x80000000u
@@ -77,6 +78,40 @@ struct PtLight {   // 32 B: a light sphere with its emission
     float4 emission;
 };
 
+// An emissive triangle of the flat list, for the extended light sampling
+// (PT_FLAG_NEE_EXTENDED): corner p0, edges, face normal, area, emission.
+struct PtTriLight {  // 64 B
+    float4 p0_area;  // p0.xyz, area
+    float4 e1_er;    // e1.xyz, emission.x
+    float4 e2_eg;    // e2.xyz, emission.y
+    float4 fn_eb;    // face normal.xyz, emission.z
+};
+
+// The extended light choice: light i (spheres of the light list first, then
+// the emissive triangles) is picked with probability
+//   pick_uniform + pick_power * power_i,
+// half uniform, half in proportion to power = luminance(emission) * area
+// (4 pi r^2 for a sphere), the uniform half keeping every light reachable.
+// Host and device compute power with these same float operations.
+#if defined(__CUDACC__)
+#define PT_HD __host__ __device__ __forceinline__
+#else
+#define PT_HD inline
+#endif
+PT_HD float pt_light_luminance(float r, float g, float b) { return 0.2126f * r + 0.7152f * g + 0.0722f * b; }
+PT_HD float pt_sphere_light_power(float lum, float radius) {
+    const float p = lum * (4.0f * 3.14159265f * (radius * radius));
+    return p > 0.0f && p < 3.0e38f ? p : 0.0f;
+}
+PT_HD float pt_triangle_area(float ax, float ay, float az, float bx, float by, float bz) {
+    const float cx = ay * bz - az * by, cy = az * bx - ax * bz, cz = ax * by - ay * bx;
+    return 0.5f * sqrtf(cx * cx + cy * cy + cz * cz);
+}
+PT_HD float pt_triangle_light_power(float lum, float area) {
+    const float p = lum * area;
+    return p > 0.0f && p < 3.0e38f ? p : 0.0f;
+}
+
 // Everything a kernel needs, passed by value.
 struct PtSceneDev {
     const float4* nodes;      // 8 float4 per node
@@ -89,6 +124,8 @@ struct PtSceneDev {
     const PtShadeInst* inst;
     const PtMaterial* mat;
     const PtLight* lights;
+    const PtTriLight* tri_lights;  // emissive flat triangles (extended light sampling)
+    const float* light_cdf;   // n_lights + n_tri_lights cumulative pick probabilities, last 1
     const float* tri_uv;      // 6 per shading triangle: texture coordinates at the corners
     const int4* tex;          // per texture: width, height, first texel float, 0
     const float* texels;      // linear RGB, 3 floats per texel, rows top first
@@ -99,6 +136,8 @@ struct PtSceneDev {
     uint32_t n_instances;
     uint32_t n_large;
     uint32_t n_lights;
+    uint32_t n_tri_lights;
+    float pick_uniform, pick_power;  // the extended pick probability of a light of power p: u + w * p
     uint32_t n_spheres;       // top-level spheres
     int sky, sample_lights, use_bvh;
     int has_textures;         // some lambertian has a texture

@@ -191,11 +191,49 @@ pt_status build_arena(const pt_scene_desc& d, HostArena& A) {
         for (uint32_t i = 0; i < d.n_spheres; ++i)
             if (emits(d.materials[d.spheres[i].material])) lights.push_back(i);
     }
+    std::vector<float> power;  // of each light, for the extended pick
     for (uint32_t l : lights) {
         const pt_sphere& s = d.spheres[l];
         const pt_material& m = d.materials[s.material];
         A.lights.push_back({make_float4(s.center[0], s.center[1], s.center[2], s.radius),
                             make_float4(m.emission[0], m.emission[1], m.emission[2], 0)});
+        power.push_back(pt_sphere_light_power(pt_light_luminance(m.emission[0], m.emission[1], m.emission[2]),
+                                              s.radius));
+    }
+    // The extended light list adds every emissive triangle of the flat list
+    // with a positive area (PT_FLAG_NEE_EXTENDED).
+    for (uint32_t i = 0; i < d.n_triangles; ++i) {
+        const pt_triangle& t = d.triangles[i];
+        const pt_material& m = d.materials[t.material];
+        if (!emits(m)) continue;
+        const float area = pt_triangle_area(t.e1[0], t.e1[1], t.e1[2], t.e2[0], t.e2[1], t.e2[2]);
+        if (!(area > 0.0f) || !(area < 3.0e38f)) continue;
+        PtTriLight L;
+        L.p0_area = make_float4(t.p0[0], t.p0[1], t.p0[2], area);
+        L.e1_er = make_float4(t.e1[0], t.e1[1], t.e1[2], m.emission[0]);
+        L.e2_eg = make_float4(t.e2[0], t.e2[1], t.e2[2], m.emission[1]);
+        L.fn_eb = make_float4(t.face_normal[0], t.face_normal[1], t.face_normal[2], m.emission[2]);
+        A.tri_lights.push_back(L);
+        power.push_back(pt_triangle_light_power(pt_light_luminance(m.emission[0], m.emission[1], m.emission[2]), area));
+    }
+    if (!power.empty()) {
+        double total = 0;
+        for (float p : power) total += p;
+        const size_t n = power.size();
+        if (total > 0) {
+            A.pick_uniform = float(0.5 / double(n));
+            A.pick_power = float(0.5 / total);
+        } else {
+            A.pick_uniform = float(1.0 / double(n));
+            A.pick_power = 0;
+        }
+        double acc = 0, sum = 0;
+        std::vector<double> pick(n);
+        for (size_t k = 0; k < n; ++k) sum += pick[k] = double(A.pick_uniform + A.pick_power * power[k]);
+        for (size_t k = 0; k < n; ++k) {
+            acc += pick[k];
+            A.light_cdf.push_back(k + 1 == n ? 1.0f : float(acc / sum));
+        }
     }
 
     for (uint32_t i = 0; i < d.n_large_spheres; ++i) {

@@ -22,6 +22,9 @@ struct HostArena {
     std::vector<PtShadeInst> inst;
     std::vector<PtMaterial> mat;
     std::vector<PtLight> lights;
+    std::vector<PtTriLight> tri_lights;  // emissive flat triangles
+    std::vector<float> light_cdf;        // extended pick: cumulative probabilities, spheres then triangles
+    float pick_uniform = 0, pick_power = 0;
     std::vector<float> tri_uv;    // 6 per shading triangle
     std::vector<int4> tex;        // width, height, first texel float, 0
     std::vector<float> texels;    // linear RGB

@@ -20,7 +20,7 @@ __device__ __forceinline__ void load_ray(const float* rays, size_t i, V& o, V& d
 template <bool FLAT>
 __global__ void __launch_bounds__(128) trace_closest_kernel(PtSceneDev S, const float* __restrict__ rays, size_t n,
                                                              float tmin, float tmax, pt_hit* __restrict__ hits) {
-    StackEntry stack[PT_STACK_MAX];
+    PT_TRAV_STACK(stack, 128);
     bool overflow = false;
     for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x) {
         V o, d;
@@ -55,7 +55,7 @@ __global__ void __launch_bounds__(128) trace_closest_kernel(PtSceneDev S, const 
 template <bool FLAT>
 __global__ void __launch_bounds__(128) trace_any_kernel(PtSceneDev S, const float* __restrict__ rays, size_t n,
                                                          float tmin, float tmax, uint8_t* __restrict__ occ) {
-    StackEntry stack[PT_STACK_MAX];
+    PT_TRAV_STACK(stack, 128);
     bool overflow = false;
     for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x) {
         V o, d;
@@ -81,7 +81,7 @@ __global__ void __launch_bounds__(128) trace_any_kernel(PtSceneDev S, const floa
 __global__ void __launch_bounds__(128) trace_count_kernel(PtSceneDev S, const float* __restrict__ rays, size_t n,
                                                            float tmin, float tmax,
                                                            unsigned long long* __restrict__ counts) {
-    StackEntry stack[PT_STACK_MAX];
+    PT_TRAV_STACK(stack, 128);
     Counts cnt = {0, 0, 0, 0, 0};
     bool overflow = false;
     for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x) {
@@ -107,7 +107,7 @@ __global__ void __launch_bounds__(128) trace_count_kernel(PtSceneDev S, const fl
 // row H - 1 - j like the frame; 0 where the ray leaves the scene.
 __global__ void __launch_bounds__(128) primary_depth_kernel(PtSceneDev S, PtCamDev C, int width, int height,
                                                              float* __restrict__ depth) {
-    StackEntry stack[PT_STACK_MAX];
+    PT_TRAV_STACK(stack, 128);
     bool overflow = false;
     const V org = mk(C.origin[0], C.origin[1], C.origin[2]), llc = mk(C.llc[0], C.llc[1], C.llc[2]);
     const V hor = mk(C.horizontal[0], C.horizontal[1], C.horizontal[2]);

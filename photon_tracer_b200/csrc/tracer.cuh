@@ -70,6 +70,79 @@ struct StackEntry {
     uint32_t pad;
 };
 
+// ---- the traversal stack -----------------------------------------------------------------
+// Entries a traversal pushes and pops (bvh.hpp:67-103: node or leaf, entry
+// distance). Each thread's entries [0, SH) live in shared memory, entries
+// [SH, PT_STACK_MAX) in a per-thread local array. The shared part is laid out
+// [depth][thread] in 16-byte entries: the lanes of a warp touch consecutive
+// 16-byte words whatever depth each lane is at, so a 128-bit access is free
+// of bank conflicts, and it is reached through a 32-bit shared-window address
+// (ld/st.shared, no generic-address check). Walks of the benchmark trees
+// rarely go deeper than SH, so their pushes and pops stay in shared memory;
+// the local array (L1-cached) takes only the deep tail, and every push is
+// still checked against PT_STACK_MAX. Measured with identical results: 8
+// entries speed the wavefront stages up 5% and the closest-hit queries 2-3%
+// (4 entries: +3% / +1%; 16: slower); kernels that keep other per-lane state
+// in shared memory choose their own count (the megakernel: 0).
+#ifndef PT_SH_STACK
+#define PT_SH_STACK 8
+#endif
+
+#ifndef PT_SH_STACK_ASM
+#define PT_SH_STACK_ASM 1
+#endif
+
+template <int SH, int NT>
+struct TravStack {
+#if PT_SH_STACK_ASM
+    uint32_t base;      // shared-window address of this thread's entry 0
+#else
+    uint4* col;         // this thread's entry 0 in the block's shared array
+#endif
+    StackEntry* deep;   // PT_STACK_MAX entries; only [SH, PT_STACK_MAX) are used
+    __device__ __forceinline__ void put(int i, StackEntry e) {
+        if (SH > 0 && i < SH) {
+#if PT_SH_STACK_ASM
+            asm volatile("st.shared.v4.u32 [%0], {%1, %2, %3, %4};" ::"r"(base + uint32_t(i) * (16u * NT)),
+                         "r"(e.first), "r"(e.count), "r"(__float_as_uint(e.t)), "r"(e.pad));
+#else
+            col[i * NT] = make_uint4(e.first, e.count, __float_as_uint(e.t), e.pad);
+#endif
+        } else {
+            deep[i] = e;
+        }
+    }
+    __device__ __forceinline__ StackEntry get(int i) const {
+        if (SH > 0 && i < SH) {
+#if PT_SH_STACK_ASM
+            uint32_t f, c, t, p;
+            asm volatile("ld.shared.v4.u32 {%0, %1, %2, %3}, [%4];"
+                         : "=r"(f), "=r"(c), "=r"(t), "=r"(p)
+                         : "r"(base + uint32_t(i) * (16u * NT)));
+            return {f, c, __uint_as_float(t), p};
+#else
+            const uint4 q = col[i * NT];
+            return {q.x, q.y, __uint_as_float(q.z), q.w};
+#endif
+        }
+        return deep[i];
+    }
+};
+
+// Declares `name`, the traversal stack of the calling thread, in a kernel of
+// NT threads per block with SH entries per thread in shared memory: the
+// block's shared part and this thread's local array.
+#if PT_SH_STACK_ASM
+#define PT_TRAV_STACK_BASE(arr) static_cast<uint32_t>(__cvta_generic_to_shared(&arr[threadIdx.x]))
+#else
+#define PT_TRAV_STACK_BASE(arr) (&arr[threadIdx.x])
+#endif
+#define PT_TRAV_STACK_N(name, NT, SH)                                                        \
+    __shared__ uint4 name##_shared[(SH) > 0 ? (SH) * (NT) : 1];                               \
+    StackEntry name##_deep[PT_STACK_MAX];                                                     \
+    ::ptd::TravStack<(SH), (NT)> name{PT_TRAV_STACK_BASE(name##_shared), name##_deep}
+#define PT_TRAV_STACK(name, NT) PT_TRAV_STACK_N(name, NT, PT_SH_STACK)
+
 // ---- primitives ------------------------------------------------------------------------
 // sphere::intersect<float> (include/sphere.hpp:25-48).
 __device__ __forceinline__ bool sphere_hit(float4 cr, V o, V d, float t_min, float& t_max) {
@@ -226,9 +299,9 @@ __device__ __forceinline__ void child_ranks(const float (&tn)[4], int mask, int 
         }
 }
 
-template <bool COUNT, class Leaf>
+template <bool COUNT, class Stack, class Leaf>
 __device__ __forceinline__ bool traverse(const PtSceneDev& S, uint32_t root, V o, V d, float t_min, float& t_max,
-                                         StackEntry* stack, int base, Counts& cnt, Leaf&& leaf) {
+                                         Stack& stack, int base, Counts& cnt, Leaf&& leaf) {
     const float4* __restrict__ nodes = S.nodes;
     const float ix = 1.0f / d.x, iy = 1.0f / d.y, iz = 1.0f / d.z;
     const bool ray_fast = PT_TRAV_FAST_MINMAX && S.ordered_boxes && finite_nonzero(ix) && finite_nonzero(iy) &&
@@ -241,13 +314,13 @@ __device__ __forceinline__ bool traverse(const PtSceneDev& S, uint32_t root, V o
     float ct = t_min;
     bool have = true;
     if (!PT_TRAV_KEEP_NEAREST) {
-        stack[top++] = {root, 0u, t_min, 0u};
+        stack.put(top++, {root, 0u, t_min, 0u});
         have = false;
     }
     while (true) {
         if (!have) {
             if (top == base) break;
-            const StackEntry e = stack[--top];
+            const StackEntry e = stack.get(--top);
             cf = e.first;
             cc = e.count;
             ct = e.t;
@@ -340,7 +413,7 @@ __device__ __forceinline__ bool traverse(const PtSceneDev& S, uint32_t root, V o
                 cc = cs[c];
                 ct = tn[c];
             } else {
-                stack[top + pos] = {fs[c], cs[c], tn[c], 0u};
+                stack.put(top + pos, {fs[c], cs[c], tn[c], 0u});
             }
         }
         top += n - kept;
@@ -390,9 +463,9 @@ struct TravRay {
 
 // Slab-tests node cf's four children against [t_min, t_max] and pushes the
 // ones hit, farthest first (bvh.hpp:72-103). False if the stack would overflow.
-template <bool COUNT>
+template <bool COUNT, class Stack>
 __device__ __forceinline__ bool expand_node(const float4* __restrict__ nodes, uint32_t cf, const TravRay& r,
-                                            float t_min, float t_max, StackEntry* stack, int& top, Counts& cnt) {
+                                            float t_min, float t_max, Stack& stack, int& top, Counts& cnt) {
     const float4* nd = nodes + 8 * size_t(cf);
     const float4 lox = __ldg(nd + r.nx), loy = __ldg(nd + r.ny), loz = __ldg(nd + r.nz);
     const float4 hix = __ldg(nd + (3 - r.nx)), hiy = __ldg(nd + (5 - r.ny)), hiz = __ldg(nd + (7 - r.nz));
@@ -449,7 +522,7 @@ __device__ __forceinline__ bool expand_node(const float4* __restrict__ nodes, ui
     child_ranks(tn, mask, rank);
 #pragma unroll
     for (int c = 0; c < 4; ++c)
-        if (mask & (1 << c)) stack[top + rank[c]] = {fs[c], cs[c], tn[c], PT_ENT_NODE};
+        if (mask & (1 << c)) stack.put(top + rank[c], {fs[c], cs[c], tn[c], PT_ENT_NODE});
     top += n;
     return true;
 }
@@ -457,18 +530,18 @@ __device__ __forceinline__ bool expand_node(const float4* __restrict__ nodes, ui
 // The BVH part of geometry::hit (ANY = false: nearest hit into h and t_max)
 // or of geometry::occluded (ANY = true: stops at the first blocker).
 // Returns bit 0 on stack overflow, bit 1 when (ANY) something blocks.
-template <bool COUNT, bool ANY>
+template <bool COUNT, bool ANY, class Stack>
 __device__ __forceinline__ int walk(const PtSceneDev& S, V wo, V wd, float t_min, float& t_max, Hit& h,
-                                    StackEntry* stack, Counts& cnt) {
+                                    Stack& stack, Counts& cnt) {
     TravRay r;
     r.set(wo, wd, t_min, S.ordered_boxes);
     uint32_t cur_inst = 0;
     bool in_mesh = false;
     int top = 0;
-    if (S.inst_root != PT_NONE) stack[top++] = {S.inst_root, 0u, t_min, PT_ENT_NODE};
-    if (S.flat_root != PT_NONE) stack[top++] = {S.flat_root, 0u, t_min, PT_ENT_NODE};
+    if (S.inst_root != PT_NONE) stack.put(top++, {S.inst_root, 0u, t_min, PT_ENT_NODE});
+    if (S.flat_root != PT_NONE) stack.put(top++, {S.flat_root, 0u, t_min, PT_ENT_NODE});
     while (top > 0) {
-        const StackEntry e = stack[--top];
+        const StackEntry e = stack.get(--top);
         uint32_t k = e.first, end = 0;
         if (e.pad == PT_ENT_WORLD) {
             r.set(wo, wd, t_min, S.ordered_boxes);
@@ -535,9 +608,9 @@ __device__ __forceinline__ int walk(const PtSceneDev& S, V wo, V wd, float t_min
             cnt.order++;
             cnt.insts++;
         }
-        if (k + 1 < end) stack[top++] = {k + 1, end, -__int_as_float(0x7f800000), PT_ENT_RESUME};
-        stack[top++] = {0u, 0u, -__int_as_float(0x7f800000), PT_ENT_WORLD};
-        stack[top++] = {meta.x, 0u, t_min, PT_ENT_NODE};
+        if (k + 1 < end) stack.put(top++, {k + 1, end, -__int_as_float(0x7f800000), PT_ENT_RESUME});
+        stack.put(top++, {0u, 0u, -__int_as_float(0x7f800000), PT_ENT_WORLD});
+        stack.put(top++, {meta.x, 0u, t_min, PT_ENT_NODE});
         r.set(aff_point(rows, wo), aff_vector(rows, wd), t_min, S.ordered_boxes);
         cur_inst = meta.y;
         in_mesh = true;
@@ -559,9 +632,9 @@ __device__ __forceinline__ int walk(const PtSceneDev& S, V wo, V wd, float t_min
 // PT_TREES_FLAT: scenes without instances; no instance-tree code at all.
 enum { PT_TREES_AUTO = 0, PT_TREES_EACH = 1, PT_TREES_ONE = 2, PT_TREES_FLAT = 3 };
 
-template <bool COUNT, int TREES = PT_TREES_AUTO>
+template <bool COUNT, int TREES = PT_TREES_AUTO, class Stack>
 __device__ __forceinline__ bool closest(const PtSceneDev& S, V o, V d, float t_min, float& t_max, Hit& h,
-                                        StackEntry* stack, Counts& cnt) {
+                                        Stack& stack, Counts& cnt) {
     h.kind = PT_HIT_NONE;
     h.index = 0;
     h.inst = 0;
@@ -675,9 +748,9 @@ __device__ __forceinline__ bool closest(const PtSceneDev& S, V o, V d, float t_m
 // the ray within [t_min, t_max]. Stops at the first blocker, which is where
 // the reference's traversal stops doing work too (it collapses t_far to t_min).
 // *overflow is set when a stack would overflow.
-template <bool COUNT, int TREES = PT_TREES_AUTO>
+template <bool COUNT, int TREES = PT_TREES_AUTO, class Stack>
 __device__ __forceinline__ bool occluded(const PtSceneDev& S, V o, V d, float t_min, float t_max,
-                                         StackEntry* stack, Counts& cnt, bool* overflow) {
+                                         Stack& stack, Counts& cnt, bool* overflow) {
     for (uint32_t i = 0; i < S.n_large; ++i) {
         float t = t_max;
         if (sphere_hit_double(__ldg(S.large + i), o, d, t_min, t)) return true;
@@ -791,8 +864,9 @@ __device__ __forceinline__ bool occluded(const PtSceneDev& S, V o, V d, float t_
 // doing work; until then both forms run the same tests with the same t_max,
 // so each returns what closest / occluded return. False when the stack
 // would overflow.
+template <class Stack>
 __device__ __forceinline__ bool query_flat(const PtSceneDev& S, V o, V d, float t_min, float& t_max, bool any,
-                                           Hit& h, StackEntry* stack) {
+                                           Hit& h, Stack& stack) {
     h.kind = PT_HIT_NONE;
     h.index = 0;
     h.inst = 0;
@@ -856,6 +930,11 @@ struct Rec {
     bool sampled_light;
     uint32_t mat;
     float tex_u, tex_v;  // texture coordinates (only filled in scenes with textures)
+    // Extended light sampling only: which light was hit (0 none, 1 a light
+    // sphere: lgeo = center, radius; 2 an emissive flat triangle: lgeo = face
+    // normal, area), for the light-sampling density of the hit direction.
+    uint32_t lkind;
+    float4 lgeo;
 };
 
 // sphere::fill (include/sphere.hpp:50-58)
@@ -907,9 +986,10 @@ __device__ __forceinline__ V sample_texture(const PtSceneDev& S, uint32_t k, flo
 // fill_instance :234-244).
 // TEX = false compiles out the texture coordinates (kernels for scenes
 // without textures: two fewer live registers through the shading code).
-template <bool TEX = true>
+template <bool TEX = true, bool EXT = false>
 __device__ __forceinline__ void fill(const PtSceneDev& S, const Hit& h, V o, V d, float t, Rec& rec) {
     rec.sampled_light = false;
+    if (EXT) rec.lkind = 0;
     rec.t = t;
     rec.tex_u = 0;
     rec.tex_v = 0;
@@ -923,12 +1003,28 @@ __device__ __forceinline__ void fill(const PtSceneDev& S, const Hit& h, V o, V d
             const uint32_t m = __ldg(&S.sph[i].mat);
             fill_sphere(cr, m, o, d, t, rec);
             rec.sampled_light = S.sample_lights && (fbits(__ldg(&S.mat[m].ior_flags.y)) & PT_MF_EMITS) != 0;
+            if (EXT && rec.sampled_light) {
+                rec.lkind = 1;
+                rec.lgeo = cr;
+            }
             break;
         }
         case PT_HIT_TRIANGLE: {
-            const uint32_t i = fbits(__ldg(S.slots + 3 * size_t(h.index) + 2).y);
+            const float4* sl = S.slots + 3 * size_t(h.index);
+            const uint32_t i = fbits(__ldg(sl + 2).y);
             rec.p = o + d * t;
             fill_triangle<TEX>(S, i, d, h.u, h.v, rec);
+            // an emissive flat triangle of positive area is a light of the extended list
+            if (EXT && S.sample_lights && (fbits(__ldg(&S.mat[rec.mat].ior_flags.y)) & PT_MF_EMITS)) {
+                const float4 a = __ldg(sl), b = __ldg(sl + 1), c = __ldg(sl + 2);
+                const float area = pt_triangle_area(a.w, b.x, b.y, b.z, b.w, c.x);
+                if (area > 0.0f && area < 3.0e38f) {
+                    const float4 fn = __ldg(&S.tri[i].fn);
+                    rec.sampled_light = true;
+                    rec.lkind = 2;
+                    rec.lgeo = make_float4(fn.x, fn.y, fn.z, area);
+                }
+            }
             break;
         }
         case PT_HIT_INSTANCE: {

@@ -211,7 +211,7 @@ __global__ void __launch_bounds__(256) wf_init(Frame F, WfView W) {
 
 // Closest hit for each queued ray.
 __global__ void __launch_bounds__(128) wf_extend(PtSceneDev S, WfView W, int cur) {
-    StackEntry stack[PT_STACK_MAX];
+    PT_TRAV_STACK(stack, 128);
     const uint32_t n = W.counts[cur];
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         W.counts[cur ^ 1] = 0;  // the next ray queue and the shadow queue start empty
@@ -328,7 +328,7 @@ __global__ void __launch_bounds__(128) wf_shade(PtSceneDev S, Frame F, WfView W,
 // The occlusion test of each shadow ray.
 template <bool AUX>
 __global__ void __launch_bounds__(128) wf_shadow(PtSceneDev S, Frame F, WfView W, int cur) {
-    StackEntry stack[PT_STACK_MAX];
+    PT_TRAV_STACK(stack, 128);
     const uint32_t n = W.counts[2];
     const int nxt = cur ^ 1;
     bool overflow = false;

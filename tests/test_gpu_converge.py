@@ -88,3 +88,24 @@ def test_next_event_estimation_matches_plain_path_tracing(pt, kind, param):
     assert np.all(se / m0 <= SE_BAR), (kind, se / m0)
     assert np.all(np.abs(m1 - m0) / m0 <= REL_BAR), (kind, m1, m0)
     assert np.all(np.abs(m1 - m0) / se <= Z_IMAGE), (kind, (m1 - m0) / se)
+
+
+def test_extended_light_sampling_matches_plain_path_tracing(pt):
+    """PT_FLAG_NEE_EXTENDED on the room lit by emissive triangle meshes (with
+    rough metal, a mirror and glass): its image converges to plain path
+    tracing's (no light sampling) within 0.1% per channel, 8 frames of
+    512x512 per setting (128 spp each)."""
+    from photon_tracer_b200 import abi
+    out = {}
+    for nee, flags in ((1, abi.PT_FLAG_NEE_EXTENDED), (0, 0)):
+        g = pt.Generated(abi.PT_GEN_MESH_LIGHT)
+        g.desc.sample_lights = nee
+        s = pt.Scene(g)
+        frames = np.array([s.render(g.camera, 512, 512, 128, 10, seed=300 + k, flags=flags)[0].reshape(-1, 3)
+                           .mean(axis=0, dtype=np.float64) for k in range(8)])
+        out[nee] = (frames.mean(axis=0), frames.std(axis=0, ddof=1) / np.sqrt(len(frames)))
+    (m1, se1), (m0, se0) = out[1], out[0]
+    se = np.sqrt(se1 ** 2 + se0 ** 2)
+    assert np.all(se / m0 <= SE_BAR), se / m0
+    assert np.all(np.abs(m1 - m0) / m0 <= REL_BAR), (m1, m0)
+    assert np.all(np.abs(m1 - m0) / se <= Z_IMAGE), (m1 - m0) / se

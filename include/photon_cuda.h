@@ -466,7 +466,8 @@ typedef struct pt_batch_info {
     int32_t threads;    /* block size of the single launch */
     int32_t tuned;
     uint64_t total_pixels, total_samples, device_bytes;
-    double tune_ms[5];  /* autotuner timings: one launch at 64/128/256 threads, per-scene megakernel, per-scene wavefront */
+    double tune_ms[8];  /* autotuner timings: one launch at 64/128/256 threads per block, per-scene megakernel,
+                           per-scene wavefront with 2^20, 2^19, 2^18 paths in flight, (unused) */
 } pt_batch_info;
 typedef struct pt_batch pt_batch;
 /* Deep-copies the scenes into one arena. PT_BATCH_AUTO measures every

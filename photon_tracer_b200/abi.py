@@ -136,7 +136,7 @@ class pt_batch_item(C.Structure):
 class pt_batch_info(C.Structure):
     _fields_ = [("n_scenes", C.c_uint32), ("strategy", C.c_int32), ("threads", C.c_int32), ("tuned", C.c_int32),
                 ("total_pixels", C.c_uint64), ("total_samples", C.c_uint64), ("device_bytes", C.c_uint64),
-                ("tune_ms", C.c_double * 5)]
+                ("tune_ms", C.c_double * 8)]
 
 
 PT_BATCH_AUTO, PT_BATCH_ONE_LAUNCH, PT_BATCH_PER_SCENE_MEGA, PT_BATCH_PER_SCENE_WAVE = 0, 1, 2, 3

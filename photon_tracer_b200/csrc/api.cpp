@@ -72,6 +72,7 @@ struct pt_scene {
     Scratch out, aux, states, in_rays, out_hits, counts, wave, sum;
     uint32_t* host_counts = nullptr;  // pinned, for the wavefront queue read-back
     int blocks_per_sm[6] = {0, 0, 0, 0, 0, 0};  // megakernel forms: aux, snapshot; extended light sampling
+    uint32_t wave_slots = 0;                   // wavefront path-queue capacity; 0: kMaxWaveSlots
 };
 
 namespace {
@@ -158,7 +159,8 @@ constexpr uint32_t kMaxWaveSlots = 1u << 20;
 pt_status launch_render(pt_scene* s, PtRenderParams& p, int mode, cudaStream_t stream) {
     if (mode == PT_MODE_WAVEFRONT) {
         const uint64_t px = uint64_t(p.width) * uint64_t(p.rows);
-        const uint32_t slots = uint32_t(px < kMaxWaveSlots ? px : kMaxWaveSlots);
+        const uint32_t cap = s->wave_slots ? s->wave_slots : kMaxWaveSlots;
+        const uint32_t slots = uint32_t(px < cap ? px : cap);
         if (pt_status e = s->wave.ensure(pt_wavefront_bytes(slots), "wavefront state")) return e;
         if (!s->host_counts)
             if (cudaError_t e = cudaMallocHost(&s->host_counts, 256)) return cuda_fail(e, "wavefront counters");
@@ -178,6 +180,12 @@ pt_status launch_render(pt_scene* s, PtRenderParams& p, int mode, cudaStream_t s
     if (cudaError_t e = pt_launch_megakernel(s->dev, p, shape, stream)) return cuda_fail(e, "megakernel launch");
     return PT_OK;
 }
+
+}  // namespace
+
+void pt::set_wave_slots(pt_scene* s, uint32_t slots) { s->wave_slots = slots; }
+
+namespace {
 
 template <class T>
 T* upload(char* base, size_t& off, const std::vector<T>& v, cudaError_t& err) {

@@ -58,8 +58,9 @@ struct pt_batch {
     cudaStream_t stream = nullptr;
     cudaGraphExec_t one_graph[3] = {nullptr, nullptr, nullptr};  // the single launch at 64, 128, 256 threads
     int strategy = PT_BATCH_AUTO, threads = 128;
+    uint32_t wave_slots = 0;  // per-scene wavefront: paths in flight (0: the library's default, 2^20)
     bool tuned = false;
-    double tune_ms[5] = {0, 0, 0, 0, 0};
+    double tune_ms[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     std::vector<cudaEvent_t> scene_events;  // per-scene completion (per-scene strategies)
     cudaEvent_t start_event = nullptr;
     cudaEvent_t done_event = nullptr;  // recorded on the render's stream after its last launch
@@ -69,7 +70,11 @@ struct pt_batch {
 namespace {
 
 std::mutex g_tune_lock;
-std::map<std::string, std::pair<int, int>> g_tune_cache;  // batch shape -> (strategy, threads)
+struct TuneChoice {
+    int strategy, threads;
+    uint32_t wave_slots;
+};
+std::map<std::string, TuneChoice> g_tune_cache;  // batch shape -> the autotuner's choice
 
 float ubits(uint32_t u) {
     float f;
@@ -244,6 +249,7 @@ pt_status run_strategy(pt_batch* b, int strategy, int threads, cudaStream_t stre
         return PT_OK;
     }
     if (strategy == PT_BATCH_PER_SCENE_MEGA) return enqueue_per_scene(b, PT_MODE_MEGAKERNEL, stream, true);
+    for (pt_scene* s : b->singles) set_wave_slots(s, b->wave_slots);
     return enqueue_per_scene(b, PT_MODE_WAVEFRONT, stream, true);
 }
 
@@ -272,23 +278,33 @@ pt_status tune(pt_batch* b) {
         std::lock_guard<std::mutex> lock(g_tune_lock);
         auto it = g_tune_cache.find(shape_key(b));
         if (it != g_tune_cache.end()) {
-            b->strategy = it->second.first;
-            b->threads = it->second.second;
+            b->strategy = it->second.strategy;
+            b->threads = it->second.threads;
+            b->wave_slots = it->second.wave_slots;
             b->tuned = true;
             return PT_OK;
         }
     }
-    // Every candidate once to warm up, then timed.
+    // Every candidate once to warm up, then timed: the single launch at three
+    // block shapes, per-scene megakernel launches, and per-scene wavefronts
+    // at three path-queue capacities.
     struct Cand {
-        int strategy, threads, slot;
+        int strategy, threads;
+        uint32_t wave_slots;
+        int slot;
     };
-    const Cand cands[5] = {{PT_BATCH_ONE_LAUNCH, 64, 0}, {PT_BATCH_ONE_LAUNCH, 128, 1}, {PT_BATCH_ONE_LAUNCH, 256, 2},
-                           {PT_BATCH_PER_SCENE_MEGA, 128, 3}, {PT_BATCH_PER_SCENE_WAVE, 128, 4}};
+    const Cand cands[7] = {{PT_BATCH_ONE_LAUNCH, 64, 0, 0},          {PT_BATCH_ONE_LAUNCH, 128, 0, 1},
+                           {PT_BATCH_ONE_LAUNCH, 256, 0, 2},         {PT_BATCH_PER_SCENE_MEGA, 128, 0, 3},
+                           {PT_BATCH_PER_SCENE_WAVE, 128, 1u << 20, 4}, {PT_BATCH_PER_SCENE_WAVE, 128, 1u << 19, 5},
+                           {PT_BATCH_PER_SCENE_WAVE, 128, 1u << 18, 6}};
+    const uint32_t keep_slots = b->wave_slots;
+    uint32_t best_slots = keep_slots;
     double best = 1e30;
     pt_status first_error = PT_OK;
     std::string first_message;
     bool any = false;
     for (const Cand& c : cands) {
+        b->wave_slots = c.wave_slots;
         double ms = time_ms(b, c.strategy, c.threads);
         if (ms >= 0) ms = time_ms(b, c.strategy, c.threads);
         if (ms < 0) {  // the candidate failed: keep the first failure's status and message
@@ -305,12 +321,14 @@ pt_status tune(pt_batch* b) {
             best = ms;
             b->strategy = c.strategy;
             b->threads = c.threads;
+            best_slots = c.wave_slots;
         }
     }
+    b->wave_slots = any ? best_slots : keep_slots;
     if (!any) return fail(first_error, first_message.c_str());
     b->tuned = true;
     std::lock_guard<std::mutex> lock(g_tune_lock);
-    g_tune_cache[shape_key(b)] = {b->strategy, b->threads};
+    g_tune_cache[shape_key(b)] = {b->strategy, b->threads, b->wave_slots};
     return PT_OK;
 }
 
@@ -530,7 +548,7 @@ pt_status pt_batch_get_info(const pt_batch* b, pt_batch_info* info) {
     info->total_pixels = b->total_pixels;
     info->total_samples = b->total_samples;
     info->device_bytes = b->arena_bytes;
-    for (int k = 0; k < 5; ++k) info->tune_ms[k] = b->tune_ms[k];
+    for (int k = 0; k < 8; ++k) info->tune_ms[k] = b->tune_ms[k];
     return PT_OK;
 }
 

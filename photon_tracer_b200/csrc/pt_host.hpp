@@ -31,6 +31,9 @@ void affine_vector(const pt_affine& x, const float v[3], float out[3]);
 void affine_point(const pt_affine& x, const float p[3], float out[3]);
 pt_affine affine_inverse(const pt_affine& x);
 uint32_t tree_depth(const std::vector<pt_bvh_node>& nodes, uint32_t root);
+// The path-queue capacity of a scene's wavefront renders (0: the default,
+// 2^20 paths in flight); the batch autotuner tries several.
+void set_wave_slots(pt_scene* s, uint32_t slots);
 
 // ---- float vector arithmetic, in the reference's evaluation order -------------------
 // (include/vec3.hpp:58-118: dot is (x*x' + y*y') + z*z', normalize divides

@@ -32,11 +32,17 @@ def param_layout():
     return out, off
 
 
-def conv_flops(batch: int, height: int, width: int) -> float:
-    """Multiply-adds x 2 of the 15 convolutions at this size (padding channels
-    included: they are computed)."""
+def conv_flops(batch: int, height: int, width: int, algorithmic: bool = False) -> float:
+    """Multiply-adds x 2 of the 15 convolutions at this size. By default the
+    padding channels are included (they are computed: the first layer's 32
+    input channels, the last layer's 16 outputs); algorithmic=True counts the
+    network's own channels instead (10 inputs, 3 outputs)."""
     total = 0.0
-    for cin, cout, level, _ in LAYERS:
+    for k, (cin, cout, level, _) in enumerate(LAYERS):
+        if algorithmic and k == 0:
+            cin = INPUT_CHANNELS
+        if algorithmic and k == len(LAYERS) - 1:
+            cout = 3
         total += 2.0 * 9 * cin * cout * batch * (height >> level) * (width >> level)
     return total
 

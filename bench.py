@@ -139,11 +139,11 @@ def l2_read_peak(stream):
         a = torch.rand(n, device="cuda")
         out = torch.empty((), device="cuda")
         for _ in range(20):
-            torch.sum(a, out=out)
+            torch.sum(a, dim=0, out=out)
         s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         s.record(stream)
         for _ in range(200):
-            torch.sum(a, out=out)
+            torch.sum(a, dim=0, out=out)
         e.record(stream)
         stream.synchronize()
     return 4 * n * 200 / (s.elapsed_time(e) / 1e3) / 1e9
@@ -377,7 +377,9 @@ def run_convergence_workload(args):
     import photon_tracer_b200 as pt
     from photon_tracer_b200 import denoiser, metrics
     w, h = 1920, 1080
-    net = denoiser.trained() if os.path.exists(denoiser.WEIGHTS) else None
+    nets = [denoiser.trained(p) for p in (args.weights or ([denoiser.WEIGHTS] if os.path.exists(denoiser.WEIGHTS)
+                                                           else []))]
+    net = nets[0] if nets else None
     results = []
     for kind in args.kinds:
         for seed in args.seeds:
@@ -394,7 +396,10 @@ def run_convergence_workload(args):
             if net is not None:
                 r["unet"] = metrics.time_to_error(scene, cam, w, h, truth, seed=seed, denoise="unet", max_spp=1024,
                                                   net=net)
-            for leg in ("atrous", "unet"):
+            for k, other in enumerate(nets[1:], 2):  # further weights files, same ground truth
+                r[f"unet{k}"] = metrics.time_to_error(scene, cam, w, h, truth, seed=seed, denoise="unet",
+                                                      max_spp=1024, net=other)
+            for leg in ["atrous", "unet"] + [f"unet{k}" for k in range(2, len(nets) + 1)]:
                 if leg in r and r[leg]["reached"] and r["plain"]["reached"]:
                     r[f"speedup_{leg}"] = round(r["plain"]["ms"] / r[leg]["ms"], 2)
             results.append(r)
@@ -576,6 +581,8 @@ def main():
     ap.add_argument("--kinds", nargs="+", default=["spheres", "room", "instances"],
                     help="convergence: scene generators (random spheres, room mesh, instancing)")
     ap.add_argument("--gt-spp", type=int, default=4096)
+    ap.add_argument("--weights", nargs="+", default=None,
+                    help="convergence: U-Net weights files (default: the committed ones); the first is 'unet'")
     ap.add_argument("--max-plain-spp", type=int, default=4096)
     ap.add_argument("--profile-case", action="store_true",
                     help="the case profiles are taken on: 1024x1024 at 4 spp, 3 frames, no baselines")

@@ -77,8 +77,13 @@ def scene_and_camera(kind: str, seed: int, aspect: float, jitter: bool):
 
 def render_pair(kind: str, seed: int, width: int, height: int, target_spp: int, jitter: bool) -> Dict:
     """One training frame: inputs at every INPUT_SPP level and the target, on the device."""
-    import torch
     g, scene, cam = scene_and_camera(kind, seed, width / height, jitter=jitter)
+    return render_view(scene, cam, kind, seed, width, height, target_spp)
+
+
+def render_view(scene: Scene, cam, kind: str, seed: int, width: int, height: int, target_spp: int) -> Dict:
+    """Inputs at every INPUT_SPP level and the target of one view of a scene, on the device."""
+    import torch
     depth = primary_depth(scene, cam, width, height)
     inputs = []
     for spp in INPUT_SPP:
@@ -87,6 +92,31 @@ def render_pair(kind: str, seed: int, width: int, height: int, target_spp: int, 
     target, _ = render(scene, cam, width, height, target_spp, seed, first_sample=TARGET_FIRST_SAMPLE, aux=False)
     scene.sync(_stream())
     return {"inputs": torch.stack(inputs).contiguous(), "target": target, "kind": kind, "seed": seed}
+
+
+def make_crop_set(kind: str, crops: int, size: int, target_spp: int, seed0: int, crops_per_scene: int,
+                  log=print) -> List[Dict]:
+    """`crops` square views of `size` of the generator `kind`: scenes from
+    seeds seed0, seed0 + 1, .., each seen through crops_per_scene jittered
+    cameras (each view's own seed drives its camera and its samples)."""
+    data = []
+    seed = seed0
+    while len(data) < crops:
+        g = Generated(SCENES[kind][0], seed=seed)
+        scene = Scene(g)
+        for v in range(min(crops_per_scene, crops - len(data))):
+            view_seed = seed * 16 + v
+            _, frm, at, vfov, scale = SCENES[kind]
+            rng = np.random.default_rng(view_seed * 7919 + 17)
+            f = np.array(frm) + rng.normal(0, scale, 3) * np.array([1.0, 0.4, 1.0])
+            a = np.array(at) + rng.normal(0, scale * 0.15, 3)
+            cam = camera_look_at(tuple(f), tuple(a), vfov * float(rng.uniform(0.75, 1.25)), 1.0)
+            t0 = time.perf_counter()
+            data.append(render_view(scene, cam, kind, view_seed, size, size, target_spp))
+            log(f"crop {kind} scene {seed} view {v}: {time.perf_counter() - t0:.2f} s")
+        scene.close()
+        seed += 1
+    return data
 
 
 def make_training_set(frames_per_kind: int, size: int, target_spp: int, seed0: int = 100,
@@ -211,6 +241,10 @@ def main(argv=None) -> int:
                    help="per-kind training frames instead of --frames/--default-frames for all kinds: "
                         "square frames from seeds SEED0.., default-camera frames from SEED0+500..")
     t.add_argument("--train-seed", type=int, default=0, help="seed of the crop sampler")
+    t.add_argument("--crops", nargs="+", default=None, metavar="KIND:COUNT:SEED0",
+                   help="square views of --size per kind instead of --mix / --frames: scenes from seeds SEED0.., "
+                        "--crops-per-scene jittered views each")
+    t.add_argument("--crops-per-scene", type=int, default=1)
     p = sub.add_parser("time")
     p.add_argument("--width", type=int, default=1920)
     p.add_argument("--height", type=int, default=1080)
@@ -235,7 +269,12 @@ def main(argv=None) -> int:
         net.sync()
         return 0
     t0 = time.perf_counter()
-    if args.mix:
+    if args.crops:
+        data = []
+        for spec in args.crops:
+            kind, count, seed0 = spec.split(":")
+            data += make_crop_set(kind, int(count), args.size, args.target_spp, int(seed0), args.crops_per_scene)
+    elif args.mix:
         data = []
         for spec in args.mix:
             kind, frames, default, seed0 = spec.split(":")

@@ -190,6 +190,42 @@ def instanced_frame(args, stream, flush, peak):
                          "note": "bytes per ray counted by the CPU oracle on 8 rows at 4 spp"}}
 
 
+def batch_summary(stream):
+    """The 64-scene batch (batch-generator seeds 1..64,
+    256^2..1024^2, 4/16/64 spp, one arena): one persistent launch from its
+    CUDA graph against one megakernel launch per scene, each rendered once to
+    warm up and then timed twice with CUDA events on `stream`; aggregate
+    samples/s and each scene's completion time. (The autotuner's full sweep
+    is --workload batch.)"""
+    import torch
+    import photon_tracer_b200 as pt
+    from photon_tracer_b200 import abi
+    t0 = time.perf_counter()
+    items = pt.batch_scenes(64)
+    build_s = time.perf_counter() - t0
+    out = {"scenes": 64, "host_scene_build_s": round(build_s, 2)}
+    for name, strategy in (("one_launch", abi.PT_BATCH_ONE_LAUNCH), ("per_scene_launches", abi.PT_BATCH_PER_SCENE_MEGA)):
+        b = pt.Batch(items, strategy)
+        b.render(stream=stream.cuda_stream)
+        ms = []
+        for _ in range(2):
+            a, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            b.render(stream=stream.cuda_stream, count_rays=False)
+            e.record(stream)
+            stream.synchronize()
+            ms.append(a.elapsed_time(e))
+        info = b.info()
+        done = b.scene_times()
+        out[name] = {"ms": round(min(ms), 1), "Msamples_s": round(info.total_samples / min(ms) / 1e3, 1),
+                     "scene_done_ms_median": round(float(np.median(done)), 1),
+                     "scene_done_ms_max": round(float(np.max(done)), 1)}
+        out["total_samples"] = int(info.total_samples)
+        b.close()
+    out["one_launch_vs_per_scene"] = round(out["per_scene_launches"]["ms"] / out["one_launch"]["ms"], 3)
+    return out
+
+
 def convergence_summary():
     """Time to relMSE <= 0.01 at 1920x1080 on one held-out seed (1001) per
     scene generator, against FP64 ground truth of 1,024 spp (its own relMSE
@@ -700,6 +736,7 @@ def main():
         l2_peak = l2_read_peak(stream)
         inst = instanced_frame(args, stream, flush, peak) if world == 1 and not args.no_extras else None
         conv = convergence_summary() if world == 1 and not args.no_extras else None
+        batch = batch_summary(stream) if world == 1 and not args.no_extras else None
         line = {
             "metric": METRIC, "value": round(value, 2), "unit": "Mrays/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(ms_per_launch, 3), "higher_is_better": True,
@@ -725,6 +762,7 @@ def main():
                                  "scene (~7 MB) is L2-resident, so frac is against HBM but served from L2"},
             "instances": inst,
             "convergence": conv,
+            "batch": batch,
             "cpu_baseline": cpu,
             "gpu_launches": args.steps,
             "clocks": clocks.summary(),

@@ -45,6 +45,15 @@ __device__ __forceinline__ unsigned long long global_ns() {
 #define PT_BATCH_ONE_QUERY 1
 #endif
 
+// As in the single-scene megakernel: each lane's pixel, sample number, scene
+// number and running sum (which change once per path) in shared memory, the
+// path itself too in the flat-scene form, and the per-scene frame values
+// (size, spp, depth, seed) read from the scene table where they are used
+// instead of held in registers for the whole loop.
+#ifndef PT_BATCH_SMEM_STATE
+#define PT_BATCH_SMEM_STATE 1
+#endif
+
 template <int THREADS, int TREES, bool TEX>
 __global__ void __launch_bounds__(THREADS, PT_BATCH_MIN_BLOCKS128 * 128 / THREADS)
     batch_megakernel(PtSceneDev S0, PtBatchLaunch B) {
@@ -55,11 +64,25 @@ __global__ void __launch_bounds__(THREADS, PT_BATCH_MIN_BLOCKS128 * 128 / THREAD
 
     unsigned long long rays = 0;
     bool exhausted = false, has_pixel = false, in_path = false, overflow = false;
-    uint32_t sc = 0;
-    int pi = 0, pj = 0, s = 0, width = 0, height = 0, spp = 0, depth = 0;
-    uint64_t seed = 0;
+#if PT_BATCH_SMEM_STATE
+    __shared__ int s_pix[4][THREADS];
+    __shared__ V s_acc[THREADS];
+    int& pi = s_pix[0][threadIdx.x];
+    int& pj = s_pix[1][threadIdx.x];
+    int& s = s_pix[2][threadIdx.x];
+    int& sci = s_pix[3][threadIdx.x];
+    V& acc = s_acc[threadIdx.x];
+    pi = pj = s = sci = 0;
+    acc = mk(0, 0, 0);
+    constexpr bool SMEM_PATH = TREES == PT_TREES_FLAT;
+#else
+    int pi = 0, pj = 0, s = 0, sci = 0;
     V acc = mk(0, 0, 0);
-    Path path;
+    constexpr bool SMEM_PATH = false;
+#endif
+    __shared__ Path s_path[SMEM_PATH ? THREADS : 1];
+    Path local_path;
+    Path& path = SMEM_PATH ? s_path[threadIdx.x] : local_path;
     First first = {mk(0, 0, 0), mk(0, 0, 0)};
     Sampler smp;
     Rng rng;
@@ -90,12 +113,11 @@ __global__ void __launch_bounds__(THREADS, PT_BATCH_MIN_BLOCKS128 * 128 / THREAD
                         if (__ldg(&B.scenes[mid].item_base) <= item) lo = mid;
                         else hi = mid - 1;
                     }
-                    sc = lo;
-                    const PtBatchScene& D = B.scenes[sc];
+                    sci = int(lo);
+                    const PtBatchScene& D = B.scenes[lo];
                     const uint32_t local = item - __ldg(&D.item_base);
                     const uint32_t tx = __ldg(&D.tiles_x);
-                    width = int(__ldg(&D.width));
-                    height = int(__ldg(&D.height));
+                    const int width = int(__ldg(&D.width)), height = int(__ldg(&D.height));
                     const uint32_t tile = local >> 5, l = local & 31u;
                     pi = int((tile % tx) * kTileW + (l & 7u));
                     pj = int((tile / tx) * kTileH + (l >> 3));
@@ -104,9 +126,6 @@ __global__ void __launch_bounds__(THREADS, PT_BATCH_MIN_BLOCKS128 * 128 / THREAD
                         s = 0;
                         in_path = false;
                         acc = mk(0, 0, 0);
-                        spp = int(__ldg(&D.spp));
-                        depth = int(__ldg(&D.depth));
-                        seed = __ldg(&D.seed);
                         S.flat_root = __ldg(&D.flat_root);
                         S.inst_root = __ldg(&D.inst_root);
                         S.large = S0.large + __ldg(&D.large_base);
@@ -123,17 +142,18 @@ __global__ void __launch_bounds__(THREADS, PT_BATCH_MIN_BLOCKS128 * 128 / THREAD
         if (__all_sync(0xffffffffu, exhausted)) break;
         if (!has_pixel) continue;
 
+        const PtBatchScene& D = B.scenes[sci];
         if (!in_path) {
-            if (depth <= 0) {
-                s = spp;
+            if (int(__ldg(&D.depth)) <= 0) {
+                s = int(__ldg(&D.spp));
             } else {
-                const PtBatchScene& D = B.scenes[sc];
                 const uint32_t idx = uint32_t(s);
+                const uint64_t seed = __ldg(&D.seed);
                 smp.begin(seed, pi, pj, idx);
                 float du, dv;
                 smp.sample_2d(0, rng, du, dv);
-                const float u = (float(pi) + du) / float(width - 1);
-                const float v = (float(pj) + dv) / float(height - 1);
+                const float u = (float(pi) + du) / float(int(__ldg(&D.width)) - 1);
+                const float v = (float(pj) + dv) / float(int(__ldg(&D.height)) - 1);
                 const V origin = mk(__ldg(&D.cam[0]), __ldg(&D.cam[1]), __ldg(&D.cam[2]));
                 const V llc = mk(__ldg(&D.cam[3]), __ldg(&D.cam[4]), __ldg(&D.cam[5]));
                 const V hor = mk(__ldg(&D.cam[6]), __ldg(&D.cam[7]), __ldg(&D.cam[8]));
@@ -151,7 +171,8 @@ __global__ void __launch_bounds__(THREADS, PT_BATCH_MIN_BLOCKS128 * 128 / THREAD
         }
 
         if constexpr (ONE_QUERY) {
-            if (in_path && query_trip<false, TEX, false>(S, path, depth, smp, rng, first, pend, shadow_pending,
+            if (in_path && query_trip<false, TEX, false>(S, path, int(__ldg(&D.depth)), smp, rng, first, pend,
+                                                         shadow_pending,
                                                   done_after_shadow, stack, rays, overflow)) {
                 acc = acc + path.rad;
                 in_path = false;
@@ -172,7 +193,8 @@ __global__ void __launch_bounds__(THREADS, PT_BATCH_MIN_BLOCKS128 * 128 / THREAD
             if (hit) fill<TEX, false>(S, h, path.o, path.d, t, rec);
             bool nee;
             Shadow sh;
-            const int step = shade<false, TEX, false>(S, path, hit, rec, depth, smp, rng, first, nee, sh, rays);
+            const int step = shade<false, TEX, false>(S, path, hit, rec, int(__ldg(&D.depth)), smp, rng, first, nee, sh,
+                                                      rays);
             if (nee) {
                 bool ovf = false;
                 if (!occluded<false, TREES>(S, sh.o, sh.d, 0.001f, sh.t_max, stack, cnt, &ovf)) path.rad = path.rad + sh.value;
@@ -185,9 +207,12 @@ __global__ void __launch_bounds__(THREADS, PT_BATCH_MIN_BLOCKS128 * 128 / THREAD
             }
         }
 
+        const int spp = int(__ldg(&D.spp));
         if (s >= spp) {
+            const int width = int(__ldg(&D.width)), height = int(__ldg(&D.height));
+            const uint32_t sc = uint32_t(sci);
             const float scale = 1.0f / float(spp);
-            float* out = B.out + __ldg(&B.scenes[sc].out_offset) + 3 * (size_t(height - 1 - pj) * width + pi);
+            float* out = B.out + __ldg(&D.out_offset) + 3 * (size_t(height - 1 - pj) * width + pi);
             out[0] = acc.x * scale;
             out[1] = acc.y * scale;
             out[2] = acc.z * scale;

@@ -94,17 +94,22 @@ def render_view(scene: Scene, cam, kind: str, seed: int, width: int, height: int
     return {"inputs": torch.stack(inputs).contiguous(), "target": target, "kind": kind, "seed": seed}
 
 
-def make_crop_set(kind: str, crops: int, size: int, target_spp: int, seed0: int, crops_per_scene: int,
-                  log=print) -> List[Dict]:
-    """`crops` square views of `size` of the generator `kind`: scenes from
-    seeds seed0, seed0 + 1, .., each seen through crops_per_scene jittered
-    cameras (each view's own seed drives its camera and its samples)."""
+def make_crop_set(kind: str, crops: int, size: int, target_spp: int, seed0: int, views_per_scene: int,
+                  tiles: int = 2, log=print) -> List[Dict]:
+    """`crops` square crops of `size` of the generator `kind`: scenes from
+    seeds seed0, seed0 + 1, .., each seen through views_per_scene jittered
+    cameras (each view's own seed drives its camera and its samples); each
+    view is rendered at (tiles * size)^2 and cut into tiles^2 crops, because
+    a frame with fewer pixels than the megakernel has lanes leaves lanes idle
+    (every lane renders a whole pixel's samples)."""
     data = []
     seed = seed0
     while len(data) < crops:
         g = Generated(SCENES[kind][0], seed=seed)
         scene = Scene(g)
-        for v in range(min(crops_per_scene, crops - len(data))):
+        for v in range(views_per_scene):
+            if len(data) >= crops:
+                break
             view_seed = seed * 16 + v
             _, frm, at, vfov, scale = SCENES[kind]
             rng = np.random.default_rng(view_seed * 7919 + 17)
@@ -112,8 +117,16 @@ def make_crop_set(kind: str, crops: int, size: int, target_spp: int, seed0: int,
             a = np.array(at) + rng.normal(0, scale * 0.15, 3)
             cam = camera_look_at(tuple(f), tuple(a), vfov * float(rng.uniform(0.75, 1.25)), 1.0)
             t0 = time.perf_counter()
-            data.append(render_view(scene, cam, kind, view_seed, size, size, target_spp))
-            log(f"crop {kind} scene {seed} view {v}: {time.perf_counter() - t0:.2f} s")
+            full = render_view(scene, cam, kind, view_seed, tiles * size, tiles * size, target_spp)
+            for ty in range(tiles):
+                for tx in range(tiles):
+                    if len(data) >= crops:
+                        break
+                    ys, xs = slice(ty * size, (ty + 1) * size), slice(tx * size, (tx + 1) * size)
+                    data.append({"inputs": full["inputs"][:, ys, xs].contiguous(),
+                                 "target": full["target"][ys, xs].contiguous(), "kind": kind, "seed": view_seed})
+            del full
+            log(f"view {kind} scene {seed} view {v}: {time.perf_counter() - t0:.2f} s")
         scene.close()
         seed += 1
     return data
@@ -242,9 +255,11 @@ def main(argv=None) -> int:
                         "square frames from seeds SEED0.., default-camera frames from SEED0+500..")
     t.add_argument("--train-seed", type=int, default=0, help="seed of the crop sampler")
     t.add_argument("--crops", nargs="+", default=None, metavar="KIND:COUNT:SEED0",
-                   help="square views of --size per kind instead of --mix / --frames: scenes from seeds SEED0.., "
-                        "--crops-per-scene jittered views each")
-    t.add_argument("--crops-per-scene", type=int, default=1)
+                   help="square crops of --size per kind instead of --mix / --frames: scenes from seeds SEED0.., "
+                        "--views-per-scene jittered views each, every view rendered at (--tiles * --size)^2 and cut "
+                        "into --tiles^2 crops")
+    t.add_argument("--views-per-scene", type=int, default=1)
+    t.add_argument("--tiles", type=int, default=2)
     p = sub.add_parser("time")
     p.add_argument("--width", type=int, default=1920)
     p.add_argument("--height", type=int, default=1080)
@@ -273,7 +288,8 @@ def main(argv=None) -> int:
         data = []
         for spec in args.crops:
             kind, count, seed0 = spec.split(":")
-            data += make_crop_set(kind, int(count), args.size, args.target_spp, int(seed0), args.crops_per_scene)
+            data += make_crop_set(kind, int(count), args.size, args.target_spp, int(seed0), args.views_per_scene,
+                                  args.tiles)
     elif args.mix:
         data = []
         for spec in args.mix:

@@ -388,6 +388,14 @@ pt_status pt_denoise_atrous_device_noalloc(int width, int height, const float* d
                                            const float* d_normal, const float* d_variance, float* d_out,
                                            void* stream);
 
+/* ---- measurement ------------------------------------------------------------------------
+ * No counterpart in the reference: the L2 read rate the traversal roofline is
+ * also reported against. Re-reads one device buffer of `bytes` (keep it
+ * under the 126 MB L2) `reps` times per launch with 16-byte loads that bypass
+ * L1; *gbs = bytes read per second over 10 launches, in GB/s. Allocates and
+ * frees its own buffer; blocking. */
+pt_status pt_measure_l2_read(size_t bytes, int reps, double* gbs);
+
 /* ---- learned denoiser (no reference counterpart) ---------------------------------
  * A U-Net over 10 guide channels per pixel: radiance 3, albedo 3, normal 3 and
  * depth 1 (the renderer's 7-float aux gives albedo and normal,

@@ -185,6 +185,7 @@ PROTOTYPES = [
     ("pt_denoise_atrous_device", ST, [C.c_int, C.c_int, P, P, P, P, P, P, P]),
     ("pt_denoise_atrous_scratch_floats", SIZE, [C.c_int, C.c_int]),
     ("pt_denoise_atrous_device_noalloc", ST, [C.c_int, C.c_int, P, P, P, P, P, P]),
+    ("pt_measure_l2_read", ST, [C.c_size_t, C.c_int, C.POINTER(C.c_double)]),
     ("pt_unet_create", ST, [C.c_uint64, C.POINTER(P)]),
     ("pt_unet_destroy", ST, [P]),
     ("pt_unet_num_params", SIZE, [P]),

@@ -240,3 +240,16 @@ def test_geometry_bridge_on_reference_scenes(pt, scene_id):
     assert res.returncode == 0 and out["hit_mismatch"] == 0, out
     assert abs(out["gpu_mean"] - out["cpu_mean"]) <= 0.02 * out["cpu_mean"], out
     assert abs(out["gpu_rays"] - out["cpu_rays"]) <= 0.02 * out["cpu_rays"], out
+
+
+def test_l2_read_probe(pt):
+    """pt_measure_l2_read: the L2 read rate the traversal roofline is reported
+    against -- a positive, finite rate, and refusals of bad arguments."""
+    import ctypes as C
+    from photon_tracer_b200 import abi
+    lib = pt.load()
+    gbs = C.c_double()
+    assert lib.pt_measure_l2_read(8 << 20, 8, C.byref(gbs)) == abi.PT_OK, lib.pt_last_error()
+    assert 100.0 < gbs.value < 1e6
+    assert lib.pt_measure_l2_read(16, 8, C.byref(gbs)) == abi.PT_ERR_INVALID_ARG
+    assert lib.pt_measure_l2_read(8 << 20, 0, C.byref(gbs)) == abi.PT_ERR_INVALID_ARG

@@ -28,10 +28,12 @@ __device__ __forceinline__ unsigned long long global_ns() {
 }
 
 // Resident 128-thread blocks per SM the register allocation targets (scaled
-// for other block sizes): 4 (at most 128 registers) measured best of 3..5 on
-// the 64-scene batch (3.42 s against 3.81 s at 3 and 3.60 s at 5).
+// for other block sizes): 5 (at most 96 registers, as the megakernel). With
+// the lane state in shared memory the 64-scene batch renders in 1,756 ms at 5
+// against 1,847 ms at 4 (identical images); before it, 4 was best (3.42 s
+// against 3.81 s at 3 and 3.60 s at 5).
 #ifndef PT_BATCH_MIN_BLOCKS128
-#define PT_BATCH_MIN_BLOCKS128 4
+#define PT_BATCH_MIN_BLOCKS128 5
 #endif
 
 // Traversal-stack entries per lane in shared memory: 0, as measured best for

@@ -30,10 +30,11 @@ reference:
   --turn 150) from the models in its checkout, in the compact form of
   tests/scene_fixture.py, with digests of the trees geometry::build made; and
   their statistical fixtures added to reference_blocks.npz;
-* ref_converge_{random_spheres,room_mesh}.npz -- the reference's own renders of
-  the 400x225 16-spp random-spheres frame and the 1024x1024 64-spp room-mesh
-  frame over 16 seeds: per-seed image means and per-20x20-block means and
-  sigmas, for the 0.1% convergence check.
+* ref_converge_{random_spheres,room_mesh,instances}.npz -- the reference's own
+  renders of the 400x225 16-spp random-spheres frame, the 1024x1024 64-spp
+  room-mesh frame and the 1920x1080 32-spp 10,000-instance frame over 16
+  seeds: per-seed image means and per-20x20-block means and sigmas, for the
+  0.1% convergence check.
 
     python tests/golden/make_golden.py [--only NAME ...]
 
@@ -191,13 +192,17 @@ def block_stats(images, block=20):
 
 # (fixture name, generator, param, width, height, spp per seed)
 CONVERGE = [("random_spheres", abi.PT_GEN_RANDOM_SPHERES, 0, 400, 225, 16),
-            ("room_mesh", abi.PT_GEN_ROOM_MESH, 6, 1024, 1024, 64)]
+            ("room_mesh", abi.PT_GEN_ROOM_MESH, 6, 1024, 1024, 64),
+            ("instances", abi.PT_GEN_INSTANCES, 0, 1920, 1080, 32)]
 CONVERGE_SEEDS = 16
 
 
 def write_convergence():
+    """Writes the convergence fixtures that are missing (delete one to write it again)."""
     threads = os.cpu_count() or 1
     for name, kind, param, w, h, spp in CONVERGE:
+        if os.path.exists(os.path.join(HERE, f"ref_converge_{name}.npz")):
+            continue
         g = pt.Generated(kind, seed=1, param=param)
         r = Reference(g.desc)
         images = []

@@ -36,11 +36,12 @@ def block_means(img, block=20):
     return img[:bh * block, :bw * block].reshape(bh, block, bw, block, 3).mean(axis=(1, 3), dtype=np.float64), bw, bh
 
 
-@pytest.mark.parametrize("name,factor", [("random_spheres", 16), ("room_mesh", 16)])
+@pytest.mark.parametrize("name,factor", [("random_spheres", 16), ("room_mesh", 16), ("instances", 16)])
 def test_converged_image_matches_reference_cpu_render(pt, name, factor):
-    """The 400x225 random-spheres frame and the 1024x1024 room-mesh frame:
-    the reference rendered each at the configuration's spp (16, 64) with 16
-    seeds; the GPU renders one frame at 16 times that spp."""
+    """The 400x225 random-spheres frame, the 1024x1024 room-mesh frame and the
+    1920x1080 10,000-instance frame: the reference rendered each at the
+    configuration's spp (16, 64, 32) with 16 seeds; the GPU renders one frame
+    at 16 times that spp."""
     f = golden(f"ref_converge_{name}.npz")
     g = pt.Generated(int(f["kind"]), seed=1, param=int(f["param"]))
     s = pt.Scene(g)

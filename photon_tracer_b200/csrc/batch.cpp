@@ -44,6 +44,7 @@ struct pt_batch {
     std::vector<PtBatchScene> scenes;
     std::vector<pt_batch_item> items;
     PtBatchScene* d_scenes = nullptr;
+    PtSceneDev* d_views = nullptr;  // per scene: the arena as that scene alone
     float* d_out = nullptr;
     size_t out_floats = 0;
     unsigned int* d_work = nullptr;
@@ -181,6 +182,7 @@ T* upload(char* base, size_t& off, const std::vector<T>& v, cudaError_t& err) {
 pt_status enqueue_one_launch(pt_batch* b, int threads, cudaStream_t stream) {
     PtBatchLaunch L;
     L.scenes = b->d_scenes;
+    L.views = b->d_views;
     L.n_scenes = uint32_t(b->scenes.size());
     L.total_items = b->total_items;
     L.out = b->d_out;
@@ -406,7 +408,7 @@ pt_status pt_batch_create(const pt_batch_item* items, uint32_t n, int32_t strate
                          align256(all.inst.size() * sizeof(PtShadeInst)) + align256(all.mat.size() * sizeof(PtMaterial)) +
                          align256(all.lights.size() * sizeof(PtLight)) + align256(all.tri_uv.size() * 4) +
                          align256(all.tex.size() * sizeof(int4)) + align256(all.texels.size() * 4) +
-                         align256(n * sizeof(PtBatchScene)) +
+                         align256(n * sizeof(PtBatchScene)) + align256(n * sizeof(PtSceneDev)) +
                          align256(out_floats * 4) + align256(n * 4) + align256(n * 8) + 4 * 256;
     cudaError_t err = cudaMalloc(&b->arena, bytes);
     if (err) return cuda_fail(err, "pt_batch_create: device allocation");
@@ -431,6 +433,8 @@ pt_status pt_batch_create(const pt_batch_item* items, uint32_t n, int32_t strate
     D.has_textures = all.has_textures;
     D.ordered_boxes = ordered_boxes(all.nodes);
     b->d_scenes = upload(base, off, b->scenes, err);
+    b->d_views = reinterpret_cast<PtSceneDev*>(base + off);
+    off += align256(n * sizeof(PtSceneDev));
     b->d_out = reinterpret_cast<float*>(base + off);
     off += align256(out_floats * 4);
     b->d_done = reinterpret_cast<unsigned int*>(base + off);
@@ -454,6 +458,26 @@ pt_status pt_batch_create(const pt_batch_item* items, uint32_t n, int32_t strate
     D.status = b->d_status;
     D.use_bvh = 1;
     D.flat_root = D.inst_root = PT_NONE;
+    {
+        // each scene's view of the merged arena: its roots, its ranges of
+        // large spheres and lights, its flags
+        std::vector<PtSceneDev> views(n, D);
+        for (uint32_t i = 0; i < n; ++i) {
+            const PtBatchScene& sc = b->scenes[i];
+            PtSceneDev& v = views[i];
+            v.flat_root = sc.flat_root;
+            v.inst_root = sc.inst_root;
+            v.large = D.large + sc.large_base;
+            v.large_mat = D.large_mat + sc.large_base;
+            v.n_large = sc.n_large;
+            v.lights = D.lights + sc.light_base;
+            v.n_lights = sc.n_lights;
+            v.sky = int(sc.sky);
+            v.sample_lights = int(sc.sample_lights);
+        }
+        err = cudaMemcpy(b->d_views, views.data(), n * sizeof(PtSceneDev), cudaMemcpyHostToDevice);
+        if (err) return cuda_fail(err, "pt_batch_create: scene views");
+    }
     if (stack_need > PT_STACK_MAX) return fail(PT_ERR_STACK_OVERFLOW, "pt_batch_create: a scene's BVH is too deep");
     // Per-scene scenes for the strategies that launch scene by scene.
     if (strategy != PT_BATCH_ONE_LAUNCH) {

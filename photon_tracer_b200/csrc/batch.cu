@@ -56,6 +56,13 @@ __device__ __forceinline__ unsigned long long global_ns() {
 #define PT_BATCH_SMEM_STATE 1
 #endif
 
+// Each scene's view of the merged arena (roots, large-sphere and light
+// ranges, flags) prebuilt in global memory and referenced by the lane's scene
+// number, instead of a copy patched per lane and held in registers.
+#ifndef PT_BATCH_SCENE_VIEWS
+#define PT_BATCH_SCENE_VIEWS 1
+#endif
+
 template <int THREADS, int TREES, bool TEX>
 __global__ void __launch_bounds__(THREADS, PT_BATCH_MIN_BLOCKS128 * 128 / THREADS)
     batch_megakernel(PtSceneDev S0, PtBatchLaunch B) {
@@ -88,7 +95,9 @@ __global__ void __launch_bounds__(THREADS, PT_BATCH_MIN_BLOCKS128 * 128 / THREAD
     First first = {mk(0, 0, 0), mk(0, 0, 0)};
     Sampler smp;
     Rng rng;
+#if !PT_BATCH_SCENE_VIEWS
     PtSceneDev S = S0;
+#endif
     // Scenes without instances: one ray query per trip, the pending shadow
     // rays in shared memory (as in the single-scene megakernel).
     constexpr bool ONE_QUERY = PT_BATCH_ONE_QUERY && TREES == PT_TREES_FLAT;
@@ -128,6 +137,7 @@ __global__ void __launch_bounds__(THREADS, PT_BATCH_MIN_BLOCKS128 * 128 / THREAD
                         s = 0;
                         in_path = false;
                         acc = mk(0, 0, 0);
+#if !PT_BATCH_SCENE_VIEWS
                         S.flat_root = __ldg(&D.flat_root);
                         S.inst_root = __ldg(&D.inst_root);
                         S.large = S0.large + __ldg(&D.large_base);
@@ -137,6 +147,7 @@ __global__ void __launch_bounds__(THREADS, PT_BATCH_MIN_BLOCKS128 * 128 / THREAD
                         S.n_lights = __ldg(&D.n_lights);
                         S.sky = int(__ldg(&D.sky));
                         S.sample_lights = int(__ldg(&D.sample_lights));
+#endif
                     }
                 }
             }
@@ -145,6 +156,9 @@ __global__ void __launch_bounds__(THREADS, PT_BATCH_MIN_BLOCKS128 * 128 / THREAD
         if (!has_pixel) continue;
 
         const PtBatchScene& D = B.scenes[sci];
+#if PT_BATCH_SCENE_VIEWS
+        const PtSceneDev& S = B.views[sci];
+#endif
         if (!in_path) {
             if (int(__ldg(&D.depth)) <= 0) {
                 s = int(__ldg(&D.spp));

@@ -22,6 +22,7 @@ struct PtBatchScene {
 
 struct PtBatchLaunch {
     const PtBatchScene* scenes;
+    const PtSceneDev* views;           // per scene: the merged arena seen as that scene alone
     uint32_t n_scenes;
     uint32_t total_items;
     float* out;

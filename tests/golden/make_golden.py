@@ -1,7 +1,8 @@
 """Writes the golden fixtures under tests/golden/ from the reference itself.
 
-Run in a checkout that has the reference (PT_REFERENCE_DIR, default
-/root/reference) with oracle/_ref built (python oracle/build.py). The
+Run in a checkout that has the reference (the directory oracle/build.py
+names: PT_REFERENCE_DIR, else its default) with oracle/_ref built
+(python oracle/build.py). The
 fixtures let the tests pin the CPU restatement on machines without the
 reference:
 
@@ -56,9 +57,9 @@ sys.path.insert(0, ROOT)
 
 import photon_tracer_b200 as pt  # noqa: E402
 from photon_tracer_b200 import abi  # noqa: E402
+from oracle.build import REFERENCE  # noqa: E402
 from oracle.oracle import Reference, reference_trees  # noqa: E402
 
-REFERENCE = os.environ.get("PT_REFERENCE_DIR", "/root/reference")
 if not os.path.isdir(os.path.join(REFERENCE, "include")):
     sys.exit(f"make_golden.py needs the reference checkout: set PT_REFERENCE_DIR (tried {REFERENCE})")
 

@@ -37,9 +37,9 @@ def test_rebuilt_scene_gives_the_reference_trees(built, name):
 
 
 def reference_model(name):
+    from oracle.build import REFERENCE
     from oracle.oracle import ref_available
-    root = os.environ.get("PT_REFERENCE_DIR", "/root/reference")
-    path = os.path.join(root, MODELS[name][1])
+    path = os.path.join(REFERENCE, MODELS[name][1])
     if not ref_available() or not os.path.exists(path):
         pytest.skip("reference checkout or harness absent")
     return path

@@ -300,6 +300,8 @@ pt_status pt_scene_create(const pt_scene_desc* desc, pt_scene** out) {
     D.texels = upload(base, off, A.texels, err);
     D.has_textures = A.has_textures;
     D.ordered_boxes = ordered_boxes(A.nodes);
+    D.stack_pack8 = stack_pack8(A.nodes);
+    D.tree_kib = tree_kib(A.nodes, A.slots);
     s->status = reinterpret_cast<unsigned int*>(base + off);
     off += 256;
     s->work = reinterpret_cast<unsigned int*>(base + off);

@@ -432,6 +432,8 @@ pt_status pt_batch_create(const pt_batch_item* items, uint32_t n, int32_t strate
     D.texels = upload(base, off, all.texels, err);
     D.has_textures = all.has_textures;
     D.ordered_boxes = ordered_boxes(all.nodes);
+    D.stack_pack8 = stack_pack8(all.nodes);
+    D.tree_kib = tree_kib(all.nodes, all.slots);
     b->d_scenes = upload(base, off, b->scenes, err);
     b->d_views = reinterpret_cast<PtSceneDev*>(base + off);
     off += align256(n * sizeof(PtSceneDev));

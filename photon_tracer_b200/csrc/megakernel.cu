@@ -63,12 +63,41 @@ constexpr int kTileW = 8, kTileH = 4;
 #define PT_MEGA_SH_STACK 0
 #endif
 
+// A second flat-scene form whose stack has 8-byte entries (PackedStack,
+// PT_TREES_FLAT8), launched for flat scenes whose leaves fit them
+// (PtSceneDev::stack_pack8) and whose nodes and leaf slots take more than
+// PT_MEGA_PACK_MIN_KIB: the deep local array is 768 instead of 1,536 bytes
+// per lane, and its hot entries take half the L1 lines. Measured on one
+// B200 with identical images (Mrays/s, 16-byte -> 8-byte): room frames with
+// the icosphere at 1,290 / 5,130 / 20,490 / 81,930 triangles (1024x1024,
+// 16 spp; about 0.1, 0.4, 1.8, 7 MB of nodes and slots) 3,191 -> 3,325 /
+// 2,921 -> 3,030 / 2,737 -> 2,827 / 2,586 -> 2,661 (+4.2 / +3.7 / +3.3 /
+// +2.9%), the 64-spp bench frame 2,608 -> 2,684; the 1080p random spheres
+// (488 spheres, about 44 KB) 4,210 -> 4,191 and 4,222 -> 4,165 in two runs
+// (-0.5 / -1.3%: the packing instructions without an L1 gain), hence the
+// threshold between the two. Shared-memory entries on top
+// (PT_MEGA_SH_STACK8 = 4, 8, 12: 4, 8, 12 KB per block) lost 4-6% on the
+// room and random-spheres frames.
+#ifndef PT_MEGA_PACK_STACK
+#define PT_MEGA_PACK_STACK 1
+#endif
+#ifndef PT_MEGA_PACK_MIN_KIB
+#define PT_MEGA_PACK_MIN_KIB 64
+#endif
+#ifndef PT_MEGA_SH_STACK8
+#define PT_MEGA_SH_STACK8 0
+#endif
+
+
 // EXT: the extended light sampling of PT_FLAG_NEE_EXTENDED (production
 // streams only); false compiles exactly the reference's estimator.
 template <bool AUX, bool SNAP, int TREES, bool TEX, bool EXT>
 __global__ void __launch_bounds__(128, PT_MEGA_MIN_BLOCKS) megakernel(PtSceneDev S, PtRenderParams P, uint32_t tiles_x,
                                                   uint32_t total_items) {
-    PT_TRAV_STACK_N(stack, 128, PT_MEGA_SH_STACK);
+    PT_FORM_STACK(stack, TREES, 128, PT_MEGA_SH_STACK, PT_MEGA_SH_STACK8);
+    // the traversal form the queries compile (PT_TREES_FLAT8 is the flat one
+    // with the other stack)
+    constexpr int QT = TREES == PT_TREES_FLAT8 ? int(PT_TREES_FLAT) : TREES;
     const int lane = threadIdx.x & 31;
     const Cam cam = {mk(P.cam.origin[0], P.cam.origin[1], P.cam.origin[2]),
                      mk(P.cam.llc[0], P.cam.llc[1], P.cam.llc[2]),
@@ -98,7 +127,7 @@ __global__ void __launch_bounds__(128, PT_MEGA_MIN_BLOCKS) megakernel(PtSceneDev
     float lum2 = 0;
     // Flat-scene form: the path (ray, throughput, radiance, bounce) in shared
     // memory too, read into registers where a query or shading needs it.
-    constexpr bool SMEM_PATH = PT_MEGA_SMEM_PATH && TREES == PT_TREES_FLAT;
+    constexpr bool SMEM_PATH = PT_MEGA_SMEM_PATH && QT == PT_TREES_FLAT;
     __shared__ Path s_path[SMEM_PATH ? 128 : 1];
     Path local_path;
     Path& path = SMEM_PATH ? s_path[threadIdx.x] : local_path;
@@ -108,7 +137,7 @@ __global__ void __launch_bounds__(128, PT_MEGA_MIN_BLOCKS) megakernel(PtSceneDev
     bool overflow = false;
     // Single-query form: the pending shadow ray (origin, direction, t_max,
     // unblocked value) of each lane, kept in shared memory between trips.
-    constexpr bool ONE_QUERY = PT_MEGA_ONE_QUERY && TREES == PT_TREES_FLAT;
+    constexpr bool ONE_QUERY = PT_MEGA_ONE_QUERY && QT == PT_TREES_FLAT;
     __shared__ float pend[10][ONE_QUERY ? 128 : 1];
     bool shadow_pending = false, done_after_shadow = false;
 
@@ -195,7 +224,7 @@ __global__ void __launch_bounds__(128, PT_MEGA_MIN_BLOCKS) megakernel(PtSceneDev
             Hit h;
             Counts cnt;
             Rec rec;
-            bool ok = closest<false, TREES>(S, path.o, path.d, 0.001f, t, h, stack, cnt);
+            bool ok = closest<false, QT>(S, path.o, path.d, 0.001f, t, h, stack, cnt);
             if (!ok) {
                 overflow = true;
                 h.kind = PT_HIT_NONE;
@@ -207,7 +236,7 @@ __global__ void __launch_bounds__(128, PT_MEGA_MIN_BLOCKS) megakernel(PtSceneDev
             const int step = shade<AUX, TEX, EXT>(S, path, hit, rec, P.depth, smp, rng, first, nee, sh, rays);
             if (nee) {
                 bool ovf = false;
-                if (!occluded<false, TREES>(S, sh.o, sh.d, 0.001f, sh.t_max, stack, cnt, &ovf))
+                if (!occluded<false, QT>(S, sh.o, sh.d, 0.001f, sh.t_max, stack, cnt, &ovf))
                     path.rad = path.rad + sh.value;
                 overflow |= ovf;
             }
@@ -287,9 +316,14 @@ int occupancy(int threads, bool aux, bool snap, bool ext) {
 }
 
 // The single-loop traversal for scenes with instances, one loop per tree
-// otherwise; texture code only in the kernels for scenes with textures.
+// otherwise; texture code only in the kernels for scenes with textures; for
+// large flat scenes without textures whose leaves fit them, 8-byte stack
+// entries.
 bool one_loop(const PtSceneDev& S) { return S.use_bvh && S.inst_root != PT_NONE; }
 bool flat_only(const PtSceneDev& S) { return S.inst_root == PT_NONE && S.n_instances == 0; }
+bool flat8(const PtSceneDev& S) {
+    return PT_MEGA_PACK_STACK && S.use_bvh && S.stack_pack8 && S.tree_kib > PT_MEGA_PACK_MIN_KIB;
+}
 
 }  // namespace
 
@@ -299,9 +333,10 @@ cudaError_t pt_launch_megakernel(const PtSceneDev& S, const PtRenderParams& p, c
         return one_loop(S)   ? launch_form<PT_TREES_ONE, true>(S, p, shape, stream)
                : flat_only(S) ? launch_form<PT_TREES_FLAT, true>(S, p, shape, stream)
                               : launch_form<PT_TREES_EACH, true>(S, p, shape, stream);
-    return one_loop(S)   ? launch_form<PT_TREES_ONE, false>(S, p, shape, stream)
-           : flat_only(S) ? launch_form<PT_TREES_FLAT, false>(S, p, shape, stream)
-                          : launch_form<PT_TREES_EACH, false>(S, p, shape, stream);
+    if (one_loop(S)) return launch_form<PT_TREES_ONE, false>(S, p, shape, stream);
+    if (!flat_only(S)) return launch_form<PT_TREES_EACH, false>(S, p, shape, stream);
+    return flat8(S) ? launch_form<PT_TREES_FLAT8, false>(S, p, shape, stream)
+                    : launch_form<PT_TREES_FLAT, false>(S, p, shape, stream);
 }
 
 int pt_megakernel_blocks_per_sm(const PtSceneDev& S, int threads, bool aux, bool snapshot, bool ext) {
@@ -309,7 +344,8 @@ int pt_megakernel_blocks_per_sm(const PtSceneDev& S, int threads, bool aux, bool
         return one_loop(S)   ? occupancy<PT_TREES_ONE, true>(threads, aux, snapshot, ext)
                : flat_only(S) ? occupancy<PT_TREES_FLAT, true>(threads, aux, snapshot, ext)
                               : occupancy<PT_TREES_EACH, true>(threads, aux, snapshot, ext);
-    return one_loop(S)   ? occupancy<PT_TREES_ONE, false>(threads, aux, snapshot, ext)
-           : flat_only(S) ? occupancy<PT_TREES_FLAT, false>(threads, aux, snapshot, ext)
-                          : occupancy<PT_TREES_EACH, false>(threads, aux, snapshot, ext);
+    if (one_loop(S)) return occupancy<PT_TREES_ONE, false>(threads, aux, snapshot, ext);
+    if (!flat_only(S)) return occupancy<PT_TREES_EACH, false>(threads, aux, snapshot, ext);
+    return flat8(S) ? occupancy<PT_TREES_FLAT8, false>(threads, aux, snapshot, ext)
+                    : occupancy<PT_TREES_FLAT, false>(threads, aux, snapshot, ext);
 }

@@ -142,4 +142,7 @@ struct PtSceneDev {
     int sky, sample_lights, use_bvh;
     int has_textures;         // some lambertian has a texture
     int ordered_boxes;        // every node child box has lo <= hi on each axis (no NaN)
+    int stack_pack8;          // every leaf holds <= 15 entries from below slot 2^26 and every
+                              // node index is below 2^31: flat-tree stack entries fit 8 bytes
+    uint32_t tree_kib;        // nodes and leaf slots of every tree, KiB (saturating)
 };

@@ -399,4 +399,27 @@ int ordered_boxes(const std::vector<float>& nodes) {
     return 1;
 }
 
+uint32_t tree_kib(const std::vector<float>& nodes, const std::vector<float>& slots) {
+    const uint64_t kib = (uint64_t(nodes.size()) + uint64_t(slots.size())) * sizeof(float) / 1024;
+    return kib > 0xffffffffu ? 0xffffffffu : uint32_t(kib);
+}
+
+// Checked over every tree of the arena (conservative: the packed entries are
+// only used by walks of a flat tree, which push flat-tree entries alone).
+int stack_pack8(const std::vector<float>& nodes) {
+    if (nodes.size() / 32 >= (size_t(1) << 31)) return 0;
+    for (size_t k = 0; k + 32 <= nodes.size(); k += 32)
+        for (int c = 0; c < 4; ++c) {
+            uint32_t first, count;
+            std::memcpy(&first, &nodes[k + 24 + c], 4);
+            std::memcpy(&count, &nodes[k + 28 + c], 4);
+            if (count == 0) {
+                if (first >= 0x80000000u) return 0;
+            } else if ((count & PT_COUNT_MASK) > 15u || first >= (1u << 26)) {
+                return 0;
+            }
+        }
+    return 1;
+}
+
 }  // namespace pt

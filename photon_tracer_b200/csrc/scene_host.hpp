@@ -41,5 +41,11 @@ pt_status build_arena(const pt_scene_desc& d, HostArena& A);
 // hi[3][4], first[4], count[4]) has lo <= hi on each axis, i.e. holds no NaN
 // and is not inverted; the traversal's fast slab test relies on it.
 int ordered_boxes(const std::vector<float>& nodes);
+// 1 when every traversal stack entry of the scene's trees fits 8 bytes
+// (PtSceneDev::stack_pack8): leaves of at most 15 primitives from below slot
+// 2^26, node indices below 2^31.
+int stack_pack8(const std::vector<float>& nodes);
+// KiB of nodes and leaf slots (PtSceneDev::tree_kib), saturating.
+uint32_t tree_kib(const std::vector<float>& nodes, const std::vector<float>& slots);
 
 }  // namespace pt

@@ -7,6 +7,8 @@
 // geometry::hit on the same rays. The comments cite the reference function
 // each routine restates (photon_tracer, include/...).
 #pragma once
+
+#include <type_traits>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -142,6 +144,65 @@ struct TravStack {
     StackEntry name##_deep[PT_STACK_MAX];                                                     \
     ::ptd::TravStack<(SH), (NT)> name{PT_TRAV_STACK_BASE(name##_shared), name##_deep}
 #define PT_TRAV_STACK(name, NT) PT_TRAV_STACK_N(name, NT, PT_SH_STACK)
+
+// The same stack in 8-byte entries, for walks of one flat tree whose leaves
+// all hold at most 15 primitives starting below slot 2^26 (PtSceneDev::
+// stack_pack8, checked when the scene is uploaded; the binned SAH builder
+// keeps leaves at <= 8 primitives except at its depth limit). An entry is
+// (word, t): an interior node is its index (bit 31 clear); a leaf sets bit
+// 31, carries PT_LEAF_HAS_SPHERE in bit 30, its count in bits 26-29 and its
+// first slot in bits 0-25. Half the bytes per entry: the shared part takes
+// 8 bytes per entry and thread ([depth][thread], a warp's 64-bit accesses
+// are conflict-free at any per-lane depth) and the local tail 768 bytes per
+// thread instead of 1,536.
+__device__ __forceinline__ uint32_t pack8_word(uint32_t first, uint32_t count) {
+    return count == 0 ? first
+                      : (0x80000000u | ((count & PT_LEAF_HAS_SPHERE) >> 1) | ((count & 15u) << 26) | first);
+}
+__device__ __forceinline__ StackEntry unpack8(uint32_t w, uint32_t t) {
+    if (w & 0x80000000u) return {w & 0x03ffffffu, ((w >> 26) & 15u) | ((w << 1) & PT_LEAF_HAS_SPHERE), __uint_as_float(t), 0u};
+    return {w, 0u, __uint_as_float(t), 0u};
+}
+
+template <int SH, int NT>
+struct PackedStack {
+    uint32_t base;  // shared-window address of this thread's entry 0
+    uint2* deep;    // PT_STACK_MAX entries; only [SH, PT_STACK_MAX) are used
+    __device__ __forceinline__ void put(int i, StackEntry e) {
+        const uint32_t w = pack8_word(e.first, e.count), t = __float_as_uint(e.t);
+        if (SH > 0 && i < SH) {
+            asm volatile("st.shared.v2.u32 [%0], {%1, %2};" ::"r"(base + uint32_t(i) * (8u * NT)), "r"(w), "r"(t));
+        } else {
+            deep[i] = make_uint2(w, t);
+        }
+    }
+    __device__ __forceinline__ StackEntry get(int i) const {
+        if (SH > 0 && i < SH) {
+            uint32_t w, t;
+            asm volatile("ld.shared.v2.u32 {%0, %1}, [%2];" : "=r"(w), "=r"(t) : "r"(base + uint32_t(i) * (8u * NT)));
+            return unpack8(w, t);
+        }
+        const uint2 q = deep[i];
+        return unpack8(q.x, q.y);
+    }
+};
+
+// Declares `name`, the traversal stack of the calling thread in a kernel of
+// form TREES with NT threads per block: 8-byte entries, SH8 of them in shared
+// memory, in the PT_TREES_FLAT8 form; 16-byte entries, SH16 in shared memory,
+// otherwise.
+#define PT_FORM_STACK(name, TREES, NT, SH16, SH8)                                                      \
+    constexpr bool name##_pack = (TREES) == ::ptd::PT_TREES_FLAT8;                                    \
+    constexpr int name##_sh16 = name##_pack ? 0 : (SH16), name##_sh8 = name##_pack ? (SH8) : 0;       \
+    __shared__ uint4 name##_s16[name##_sh16 > 0 ? name##_sh16 * (NT) : 1];                            \
+    __shared__ uint2 name##_s8[name##_sh8 > 0 ? name##_sh8 * (NT) : 1];                               \
+    std::conditional_t<name##_pack, uint2, ::ptd::StackEntry> name##_deep[PT_STACK_MAX];              \
+    std::conditional_t<name##_pack, ::ptd::PackedStack<name##_sh8, (NT)>,                             \
+                       ::ptd::TravStack<name##_sh16, (NT)>>                                           \
+        name{static_cast<uint32_t>(__cvta_generic_to_shared(name##_pack ? static_cast<void*>(&name##_s8[0])  \
+                                                                        : static_cast<void*>(&name##_s16[0]))) + \
+                 threadIdx.x * (name##_pack ? 8u : 16u),                                                \
+             name##_deep}
 
 // ---- primitives ------------------------------------------------------------------------
 // sphere::intersect<float> (include/sphere.hpp:25-48).
@@ -630,7 +691,10 @@ __device__ __forceinline__ int walk(const PtSceneDev& S, V wo, V wd, float t_min
 // the two single forms and the host launches the one for its scene, so a
 // flat scene's kernel carries no two-level code.
 // PT_TREES_FLAT: scenes without instances; no instance-tree code at all.
-enum { PT_TREES_AUTO = 0, PT_TREES_EACH = 1, PT_TREES_ONE = 2, PT_TREES_FLAT = 3 };
+// PT_TREES_FLAT8: a kernel form, not a query form -- PT_TREES_FLAT with the
+// traversal stack in 8-byte entries (PackedStack); the kernel passes
+// PT_TREES_FLAT to the queries.
+enum { PT_TREES_AUTO = 0, PT_TREES_EACH = 1, PT_TREES_ONE = 2, PT_TREES_FLAT = 3, PT_TREES_FLAT8 = 4 };
 
 template <bool COUNT, int TREES = PT_TREES_AUTO, class Stack>
 __device__ __forceinline__ bool closest(const PtSceneDev& S, V o, V d, float t_min, float& t_max, Hit& h,

@@ -235,8 +235,10 @@ def convergence_summary():
             if leg == "unet" and net is None:
                 continue
             t = metrics.time_to_error(scene, cam, w, h, truth, seed=1001, **kw)
+            last = t["history"][-1] if t.get("history") else {}
             r[leg] = {"spp": t["spp"], "ms": None if t["ms"] is None else round(t["ms"], 2),
-                      "relmse": round(t["relmse"], 5)}
+                      "relmse": round(t["relmse"], 5),
+                      "ssim": None if last.get("ssim") is None else round(float(last["ssim"]), 4)}
         for leg in ("atrous", "unet"):
             if leg in r and r[leg]["ms"] and r["plain"]["ms"]:
                 r[f"speedup_{leg}"] = round(r["plain"]["ms"] / r[leg]["ms"], 2)

@@ -396,6 +396,29 @@ def run_batch_workload(args):
     return 0
 
 
+def extend_ground_truth(gt, args, kind, seed, t0):
+    """Resumes the checkpoint of this frame from args.gt_cache (when there is
+    one) and adds 256-spp passes up to args.gt_spp, saving every 16 passes and
+    at the end, and stopping early once args.gt_budget_s seconds have passed
+    since t0. Returns whether the ground truth reached args.gt_spp."""
+    os.makedirs(args.gt_cache, exist_ok=True)
+    tag = f"{kind}:{seed}"
+    path = os.path.join(args.gt_cache, f"gt_{kind}_{seed}_{gt.w}x{gt.h}.npz")
+    if os.path.exists(path):
+        gt.resume(path, tag)
+    added = 0
+    while gt.spp < args.gt_spp:
+        if args.gt_budget_s is not None and time.perf_counter() - t0 > args.gt_budget_s:
+            break
+        gt.add(1)
+        added += 1
+        if added % 16 == 0:
+            gt.save(path, tag)
+    if added:
+        gt.save(path, tag)
+    return gt.spp >= args.gt_spp
+
+
 def run_convergence_workload(args):
     """The headline study at 1920x1080: time to reach relMSE <= 0.01 against
     FP64 ground truth for plain path tracing, for path tracing followed by the
@@ -413,7 +436,15 @@ def run_convergence_workload(args):
             g, scene, cam = denoiser.scene_and_camera(kind, seed, w / h, jitter=False)
             gt = metrics.GroundTruth(scene, cam, w, h, seed=seed, pass_spp=256)
             t = time.perf_counter()
-            gt.add(max(1, args.gt_spp // 256))
+            if args.gt_cache is None:
+                gt.add(max(1, args.gt_spp // 256))
+            else:
+                complete = extend_ground_truth(gt, args, kind, seed, t)
+                if args.gt_only or not complete:
+                    print(json.dumps({"ground_truth": f"{kind}:{seed}", "spp": gt.spp, "target_spp": args.gt_spp,
+                                      "s": round(time.perf_counter() - t, 1)}), flush=True)
+                    scene.close()
+                    continue
             gt_s = time.perf_counter() - t
             truth = gt.image()
             r = {"kind": kind, "seed": seed, "gt_spp": gt.spp, "gt_s": round(gt_s, 2)}
@@ -608,6 +639,14 @@ def main():
     ap.add_argument("--kinds", nargs="+", default=["spheres", "room", "instances"],
                     help="convergence: scene generators (random spheres, room mesh, instancing)")
     ap.add_argument("--gt-spp", type=int, default=4096)
+    ap.add_argument("--gt-cache", default=None,
+                    help="convergence: directory of ground-truth checkpoints (FP64 sums); a frame's checkpoint is "
+                         "resumed and extended to --gt-spp, then saved, so a long ground truth can be built over "
+                         "several runs")
+    ap.add_argument("--gt-only", action="store_true",
+                    help="convergence: only build or extend the ground-truth checkpoints (with --gt-cache)")
+    ap.add_argument("--gt-budget-s", type=float, default=None,
+                    help="convergence: stop extending a ground truth after this many seconds (with --gt-cache)")
     ap.add_argument("--weights", nargs="+", default=None,
                     help="convergence: U-Net weights files (default: the committed ones); the first is 'unet'")
     ap.add_argument("--max-plain-spp", type=int, default=4096)

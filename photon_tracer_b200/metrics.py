@@ -5,6 +5,9 @@
 * GroundTruth: per-pixel radiance sums in FP64 over progressive passes on the
   GPU (pt_render_device with first_sample continuing the per-pixel sample
   numbering, pt_accumulate_pass adding each pass's averages * spp in double).
+  save() / resume() checkpoint the sums, so a long ground truth (65,536 spp at
+  1920x1080 is minutes per frame) can be built over several runs; a resumed
+  run continues the sample numbers, so its sums equal an uninterrupted run's.
 * time_to_error: the smallest power-of-two spp whose image reaches a relMSE
   target against ground truth, for plain path tracing and for path tracing
   followed by a denoiser (the a-trous filter or the learned U-Net), with the
@@ -13,6 +16,7 @@
 from __future__ import annotations
 
 import ctypes as C
+import os
 from typing import Callable, Optional
 
 import numpy as np
@@ -79,6 +83,43 @@ class GroundTruth:
 
     def image(self) -> np.ndarray:
         return (self.sum / self.spp).cpu().numpy()
+
+    # What a checkpoint must agree on to continue the same sums.
+    _KEYS = ("width", "height", "seed", "depth", "pass_spp", "first")
+
+    def _fields(self) -> dict:
+        return {"width": self.w, "height": self.h, "seed": self.seed, "depth": self.depth,
+                "pass_spp": self.pass_spp, "first": self.first}
+
+    def save(self, path: str, tag: str = "") -> None:
+        """Writes the FP64 sums, the samples they hold and the frame they belong
+        to (`tag` names the scene, e.g. "room:1001") to `path` (.npz), through a
+        temporary file renamed into place."""
+        tmp = path + ".tmp"
+        with open(tmp, "wb") as f:
+            np.savez(f, sum=self.sum.cpu().numpy(), spp=np.int64(self.spp), tag=np.str_(tag),
+                     **{k: np.int64(v) for k, v in self._fields().items()})
+        os.replace(tmp, path)
+
+    def resume(self, path: str, tag: str = "") -> None:
+        """Loads a checkpoint save() wrote for the same frame and scene; later
+        add() calls continue its sample numbers. Raises ValueError when the
+        checkpoint belongs to another frame, scene or sampling."""
+        import torch
+        with np.load(path, allow_pickle=False) as f:
+            if str(f["tag"]) != tag:
+                raise ValueError(f"{path}: checkpoint of scene {str(f['tag'])!r}, not {tag!r}")
+            for k, mine in self._fields().items():
+                if int(f[k]) != int(mine):
+                    raise ValueError(f"{path}: checkpoint {k} = {int(f[k])}, this ground truth has {mine}")
+            s = f["sum"]
+            if s.dtype != np.float64 or s.shape != tuple(self.sum.shape):
+                raise ValueError(f"{path}: sums of {s.dtype} {s.shape}, expected float64 {tuple(self.sum.shape)}")
+            spp = int(f["spp"])
+            if spp < 0 or spp % self.pass_spp:
+                raise ValueError(f"{path}: {spp} samples is not a whole number of {self.pass_spp}-sample passes")
+            self.sum.copy_(torch.from_numpy(np.ascontiguousarray(s)))
+            self.spp = spp
 
 
 def _timed(fn: Callable[[], None]) -> float:

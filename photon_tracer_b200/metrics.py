@@ -118,7 +118,11 @@ class GroundTruth:
             spp = int(f["spp"])
             if spp < 0 or spp % self.pass_spp:
                 raise ValueError(f"{path}: {spp} samples is not a whole number of {self.pass_spp}-sample passes")
+            if self.sum.is_cuda:  # nothing of this ground truth's may still be running on any stream
+                torch.cuda.synchronize(self.sum.device)
             self.sum.copy_(torch.from_numpy(np.ascontiguousarray(s)))
+            if self.sum.is_cuda:
+                torch.cuda.synchronize(self.sum.device)
             self.spp = spp
 
 

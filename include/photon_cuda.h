@@ -416,6 +416,9 @@ typedef struct pt_unet pt_unet;
 pt_status pt_unet_create(uint64_t seed, pt_unet** out);
 pt_status pt_unet_destroy(pt_unet* net);
 size_t pt_unet_num_params(const pt_unet* net);
+/* Copy the float parameters out / in (pt_unet_num_params floats). Both wait
+ * for all work on the device first, so a training step in flight on any
+ * stream finishes before the copy; blocking. */
 pt_status pt_unet_get_params(const pt_unet* net, float* host_params);
 pt_status pt_unet_set_params(pt_unet* net, const float* host_params);
 /* 1 (default): convolutions with bfloat16 inputs run on the tensor cores where

@@ -550,13 +550,15 @@ pt_status pt_batch_scene_times(pt_batch* b, double* ms) {
     if (b->last_strategy == PT_BATCH_ONE_LAUNCH) {
         std::vector<unsigned long long> done(n);
         unsigned long long start = 0;
-        cudaMemcpy(done.data(), b->d_done_ns, n * 8, cudaMemcpyDeviceToHost);
-        cudaMemcpy(&start, b->d_start, 8, cudaMemcpyDeviceToHost);
+        cudaError_t e = cudaMemcpy(done.data(), b->d_done_ns, n * 8, cudaMemcpyDeviceToHost);
+        if (!e) e = cudaMemcpy(&start, b->d_start, 8, cudaMemcpyDeviceToHost);
+        if (e) return cuda_fail(e, "pt_batch_scene_times");
         for (size_t i = 0; i < n; ++i) ms[i] = done[i] >= start ? double(done[i] - start) * 1e-6 : 0.0;
     } else {
         for (size_t i = 0; i < n; ++i) {
             float t = 0;
-            cudaEventElapsedTime(&t, b->start_event, b->scene_events[i]);
+            if (cudaError_t e = cudaEventElapsedTime(&t, b->start_event, b->scene_events[i]))
+                return cuda_fail(e, "pt_batch_scene_times");
             ms[i] = t;
         }
     }

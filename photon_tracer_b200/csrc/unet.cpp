@@ -369,15 +369,18 @@ size_t pt_unet_num_params(const pt_unet* n) { return n ? n->n_params : 0; }
 pt_status pt_unet_get_params(const pt_unet* n, float* host) {
     clear_error();
     if (!n || !host) return fail(PT_ERR_INVALID_ARG, "pt_unet_get_params: null pointer");
-    if (cudaError_t e = cudaMemcpy(host, n->params.p, n->n_params * 4, cudaMemcpyDeviceToHost))
-        return cuda_fail(e, "pt_unet_get_params");
-    return PT_OK;
+    // a training step may still be running on a non-blocking stream, which
+    // the copy below would not wait for
+    cudaError_t e = cudaDeviceSynchronize();
+    if (!e) e = cudaMemcpy(host, n->params.p, n->n_params * 4, cudaMemcpyDeviceToHost);
+    return e ? cuda_fail(e, "pt_unet_get_params") : PT_OK;
 }
 
 pt_status pt_unet_set_params(pt_unet* n, const float* host) {
     clear_error();
     if (!n || !host) return fail(PT_ERR_INVALID_ARG, "pt_unet_set_params: null pointer");
-    cudaError_t e = cudaMemcpy(n->params.p, host, n->n_params * 4, cudaMemcpyHostToDevice);
+    cudaError_t e = cudaDeviceSynchronize();  // as in pt_unet_get_params
+    if (!e) e = cudaMemcpy(n->params.p, host, n->n_params * 4, cudaMemcpyHostToDevice);
     if (!e) e = unet::f32_to_bf16(long(n->n_params), n->params.as<float>(), n->params16.as<__nv_bfloat16>(), nullptr);
     if (!e) e = cudaDeviceSynchronize();
     return e ? cuda_fail(e, "pt_unet_set_params") : PT_OK;
